@@ -1,0 +1,751 @@
+// C ABI of libparw2v: context management, set-up and the training dispatch (include/parw2v.h).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "internal.h"
+
+using namespace parw2v;
+
+struct parw2v_ctx {
+    parw2v_config cfg{};
+    int ld = 0;
+    bool bf16 = false;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+    std::string err;
+    size_t allocated = 0;
+    std::vector<void *> owned;
+    // vocabulary and tables
+    int vocab = 0;
+    uint64_t train_words = 0;
+    uint32_t *d_counts = nullptr;
+    int32_t *d_table = nullptr;
+    float *d_exp = nullptr;
+    float *d_thr = nullptr;
+    // weights
+    void *d_w_in = nullptr, *d_w_out = nullptr;
+    bool weights_ready = false;
+    // corpus and packing
+    int32_t *d_corpus = nullptr;
+    uint64_t n_tokens = 0, corpus_cap = 0;
+    int32_t *d_packed = nullptr;
+    uint32_t *d_line_end = nullptr;
+    uint64_t line_cap = 0;
+    uint32_t *d_tile_kept = nullptr, *d_tile_zero = nullptr;
+    uint64_t tile_cap = 0;
+    // workspace
+    float *d_scratch = nullptr;
+    size_t scratch_floats = 0;
+    DevCounters *d_cnt = nullptr;
+    // trace
+    parw2v_trace *trace = nullptr;
+    DevTrace dtr;
+    size_t trace_bytes = 0;
+    void *d_trace_mem = nullptr;
+};
+
+static std::string g_create_error;
+
+static int fail(parw2v_ctx *c, int code, const std::string &msg) {
+    if (c) c->err = msg;
+    else g_create_error = msg;
+    return code;
+}
+
+static int cuda_fail(parw2v_ctx *c, cudaError_t e, const char *what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    if (e == cudaErrorMemoryAllocation) return fail(c, PARW2V_ERR_OOM, m);
+    return fail(c, PARW2V_ERR_CUDA, m);
+}
+
+#define CK(c, call, what)                               \
+    do {                                                \
+        cudaError_t e_ = (call);                        \
+        if (e_ != cudaSuccess) return cuda_fail(c, e_, what); \
+    } while (0)
+
+// Device allocation against the context's memory cap.
+static int dalloc(parw2v_ctx *c, void **p, size_t bytes, const char *what) {
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    if (c->cfg.mem_cap_bytes && c->allocated + bytes > c->cfg.mem_cap_bytes)
+        return fail(c, PARW2V_ERR_OOM, std::string(what) + ": exceeds mem_cap_bytes");
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return cuda_fail(c, e, what);
+    }
+    c->allocated += bytes;
+    c->owned.push_back(*p);
+    return PARW2V_OK;
+}
+
+static void dfree(parw2v_ctx *c, void *p, size_t bytes) {
+    if (!p) return;
+    for (size_t i = 0; i < c->owned.size(); i++)
+        if (c->owned[i] == p) {
+            c->owned.erase(c->owned.begin() + (long) i);
+            break;
+        }
+    cudaFree(p);
+    c->allocated -= bytes < c->allocated ? bytes : c->allocated;
+}
+
+static int set_device(parw2v_ctx *c) {
+    CK(c, cudaSetDevice(c->cfg.device), "cudaSetDevice");
+    return PARW2V_OK;
+}
+
+static size_t welem(const parw2v_ctx *c) { return c->bf16 ? sizeof(__nv_bfloat16) : sizeof(float); }
+
+extern "C" {
+
+const char *parw2v_version(void) { return "parw2v-b200 0.1 (sm_100a)"; }
+
+const char *parw2v_strerror(int s) {
+    switch (s) {
+        case PARW2V_OK: return "ok";
+        case PARW2V_ERR_ARG: return "invalid argument";
+        case PARW2V_ERR_CUDA: return "CUDA error";
+        case PARW2V_ERR_OOM: return "out of device memory";
+        case PARW2V_ERR_CAPACITY: return "input exceeds a library limit";
+        case PARW2V_ERR_TIMEOUT: return "bounded device loop gave up";
+        case PARW2V_ERR_STATE: return "call order violated";
+        case PARW2V_ERR_IO: return "file I/O error";
+        case PARW2V_ERR_NODEV: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+
+const char *parw2v_last_error(const parw2v_ctx *c) { return c ? c->err.c_str() : g_create_error.c_str(); }
+
+int parw2v_create(const parw2v_config *cfg, parw2v_ctx **out) {
+    if (!cfg || !out) return fail(nullptr, PARW2V_ERR_ARG, "null argument");
+    *out = nullptr;
+    const parw2v_config &k = *cfg;
+    if (k.size < 1 || k.window < 1 || k.negative < 0 || k.batch_size < 1 || k.iter < 1 || !(k.alpha > 0) ||
+        k.sample < 0 || k.mode < PARW2V_MODE_DET || k.mode > PARW2V_MODE_BATCHED_BF16 || k.grid < 0 ||
+        k.warps_per_cta < 0)
+        return fail(nullptr, PARW2V_ERR_ARG, "invalid configuration value");
+    if (k.window > 100 || k.negative > 100 || k.batch_size > 1000)
+        return fail(nullptr, PARW2V_ERR_CAPACITY, "window/negative/batch_size beyond the supported range");
+    if (k.mode != PARW2V_MODE_DET && k.size > 512)
+        return fail(nullptr, PARW2V_ERR_CAPACITY, "Hogwild modes support size <= 512");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(nullptr, PARW2V_ERR_NODEV, "no CUDA device available");
+    }
+    if (k.device < 0 || k.device >= ndev) return fail(nullptr, PARW2V_ERR_ARG, "device ordinal out of range");
+    parw2v_ctx *c = new parw2v_ctx();
+    c->cfg = k;
+    c->bf16 = (k.mode == PARW2V_MODE_BATCHED_BF16);
+    const int align = c->bf16 ? 8 : 4;  // 16-byte rows
+    c->ld = (k.size + align - 1) / align * align;
+    int rc = set_device(c);
+    if (rc == PARW2V_OK) {
+        cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
+        if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
+        if (e == cudaSuccess) e = cudaEventCreate(&c->ev2);
+        if (e != cudaSuccess) rc = cuda_fail(c, e, "stream/event creation");
+    }
+    if (rc == PARW2V_OK) rc = dalloc(c, (void **) &c->d_cnt, sizeof(DevCounters), "counters");
+    if (rc == PARW2V_OK) rc = dalloc(c, (void **) &c->d_exp, sizeof(float) * (kExpTableSize + 1), "expTable");
+    if (rc != PARW2V_OK) {
+        g_create_error = c->err;
+        parw2v_destroy(c);
+        return rc;
+    }
+    // expTable on the host with the reference's float expression (PAR_Word2Vec_cpu.cpp:822-826;
+    // exp of a float argument is expf in the reference's C++)
+    float h_exp[kExpTableSize + 1];
+    for (int i = 0; i < kExpTableSize + 1; i++) {
+        float x = ((float) i / (float) kExpTableSize * 2.0f - 1.0f) * (float) kMaxExp;
+        float e = expf(x);
+        h_exp[i] = e / (e + 1.0f);
+    }
+    cudaError_t e = cudaMemcpyAsync(c->d_exp, h_exp, sizeof(h_exp), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+        rc = cuda_fail(c, e, "expTable upload");
+        g_create_error = c->err;
+        parw2v_destroy(c);
+        return rc;
+    }
+    *out = c;
+    return PARW2V_OK;
+}
+
+void parw2v_destroy(parw2v_ctx *c) {
+    if (!c) return;
+    cudaSetDevice(c->cfg.device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (void *p : c->owned) cudaFree(p);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->ev2) cudaEventDestroy(c->ev2);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+int parw2v_set_vocab(parw2v_ctx *c, const uint32_t *counts, int V) {
+    if (!c || !counts) return fail(c, PARW2V_ERR_ARG, "null argument");
+    if (V < 2) return fail(c, PARW2V_ERR_ARG, "vocab_size must be >= 2 (\"</s>\" plus one word)");
+    int rc = set_device(c);
+    if (rc) return rc;
+    if (c->vocab != V) {
+        dfree(c, c->d_counts, sizeof(uint32_t) * (size_t) c->vocab);
+        dfree(c, c->d_thr, sizeof(float) * (size_t) c->vocab);
+        c->d_counts = nullptr;
+        c->d_thr = nullptr;
+        if (c->d_w_in) {
+            dfree(c, c->d_w_in, welem(c) * (size_t) c->vocab * c->ld);
+            dfree(c, c->d_w_out, welem(c) * (size_t) c->vocab * c->ld);
+            c->d_w_in = c->d_w_out = nullptr;
+        }
+        c->weights_ready = false;
+        if ((rc = dalloc(c, (void **) &c->d_counts, sizeof(uint32_t) * (size_t) V, "counts"))) return rc;
+        if ((rc = dalloc(c, (void **) &c->d_thr, sizeof(float) * (size_t) V, "thresholds"))) return rc;
+        c->vocab = V;
+    }
+    if (!c->d_table && (rc = dalloc(c, (void **) &c->d_table, sizeof(int32_t) * (size_t) kTableSize, "table")))
+        return rc;
+    uint64_t tw = 0;
+    for (int i = 0; i < V; i++) tw += counts[i];
+    c->train_words = tw;
+    // cn^0.75 as the reference computes it: pow(unsigned, float) promotes both to double
+    std::vector<double> pw((size_t) V);
+    for (int i = 0; i < V; i++) pw[(size_t) i] = pow((double) counts[i], (double) 0.75f);
+    void *tmp = nullptr;
+    const size_t tmp_bytes = sizeof(double) * (size_t) V + sizeof(float) * (size_t) V + sizeof(long long) * (size_t) V +
+                             sizeof(double) + 16;  // + alignment slack for the int64 array
+    if ((rc = dalloc(c, &tmp, tmp_bytes, "table workspace"))) return rc;
+    double *d_pow = (double *) tmp;
+    float *d_D = (float *) (d_pow + V);
+    long long *d_g = (long long *) (((uintptr_t) (d_D + V) + 7) & ~(uintptr_t) 7);
+    double *d_total = (double *) (d_g + V);
+    cudaError_t e = cudaMemcpyAsync(d_pow, pw.data(), sizeof(double) * (size_t) V, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c->d_counts, counts, sizeof(uint32_t) * (size_t) V, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = launch_build_table(d_pow, V, c->d_table, d_D, d_g, d_total, c->stream);
+    if (e == cudaSuccess) e = launch_build_thresholds(c->d_counts, V, c->cfg.sample, tw, c->d_thr, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    dfree(c, tmp, tmp_bytes);
+    if (e != cudaSuccess) return cuda_fail(c, e, "unigram table / thresholds");
+    return PARW2V_OK;
+}
+
+int parw2v_get_table(parw2v_ctx *c, int32_t *table) {
+    if (!c || !table) return fail(c, PARW2V_ERR_ARG, "null argument");
+    if (!c->vocab) return fail(c, PARW2V_ERR_STATE, "set_vocab first");
+    int rc = set_device(c);
+    if (rc) return rc;
+    CK(c, cudaMemcpyAsync(table, c->d_table, sizeof(int32_t) * (size_t) kTableSize, cudaMemcpyDeviceToHost, c->stream),
+       "table download");
+    CK(c, cudaStreamSynchronize(c->stream), "table download");
+    return PARW2V_OK;
+}
+
+int parw2v_get_exp_table(parw2v_ctx *c, float *t) {
+    if (!c || !t) return fail(c, PARW2V_ERR_ARG, "null argument");
+    int rc = set_device(c);
+    if (rc) return rc;
+    CK(c, cudaMemcpyAsync(t, c->d_exp, sizeof(float) * (kExpTableSize + 1), cudaMemcpyDeviceToHost, c->stream),
+       "expTable download");
+    CK(c, cudaStreamSynchronize(c->stream), "expTable download");
+    return PARW2V_OK;
+}
+
+static int ensure_weights(parw2v_ctx *c) {
+    if (!c->vocab) return fail(c, PARW2V_ERR_STATE, "set_vocab first");
+    if (c->d_w_in) return PARW2V_OK;
+    const size_t bytes = welem(c) * (size_t) c->vocab * c->ld;
+    int rc = dalloc(c, &c->d_w_in, bytes, "W_in");
+    if (!rc) rc = dalloc(c, &c->d_w_out, bytes, "W_out");
+    return rc;
+}
+
+int parw2v_init_weights(parw2v_ctx *c) {
+    if (!c) return fail(c, PARW2V_ERR_ARG, "null argument");
+    int rc = set_device(c);
+    if (!rc) rc = ensure_weights(c);
+    if (rc) return rc;
+    cudaError_t e;
+    if (c->bf16)
+        e = launch_init_net(nullptr, nullptr, (__nv_bfloat16 *) c->d_w_in, (__nv_bfloat16 *) c->d_w_out, c->vocab,
+                            c->cfg.size, c->ld, c->stream);
+    else
+        e = launch_init_net((float *) c->d_w_in, (float *) c->d_w_out, nullptr, nullptr, c->vocab, c->cfg.size, c->ld,
+                            c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "InitNet");
+    c->weights_ready = true;
+    return PARW2V_OK;
+}
+
+// Host [V][d] FP32 <-> device [V][ld] rows, through a pitched copy (and a BF16 conversion).
+static int copy_weights(parw2v_ctx *c, const float *src_h, float *dst_h, void *dev) {
+    const size_t V = (size_t) c->vocab, d = (size_t) c->cfg.size, ld = (size_t) c->ld;
+    if (!c->bf16) {
+        if (src_h) {
+            CK(c, cudaMemsetAsync(dev, 0, sizeof(float) * V * ld, c->stream), "weights clear");
+            CK(c, cudaMemcpy2DAsync(dev, ld * sizeof(float), src_h, d * sizeof(float), d * sizeof(float), V,
+                                    cudaMemcpyHostToDevice, c->stream), "weights upload");
+        } else {
+            CK(c, cudaMemcpy2DAsync(dst_h, d * sizeof(float), dev, ld * sizeof(float), d * sizeof(float), V,
+                                    cudaMemcpyDeviceToHost, c->stream), "weights download");
+        }
+        CK(c, cudaStreamSynchronize(c->stream), "weights copy");
+        return PARW2V_OK;
+    }
+    void *tmp = nullptr;
+    const size_t bytes = sizeof(float) * V * ld;
+    int rc = dalloc(c, &tmp, bytes, "weights staging");
+    if (rc) return rc;
+    cudaError_t e = cudaSuccess;
+    if (src_h) {
+        e = cudaMemsetAsync(tmp, 0, bytes, c->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(tmp, ld * sizeof(float), src_h, d * sizeof(float), d * sizeof(float), V,
+                                  cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess) e = launch_narrow_bf16((float *) tmp, (__nv_bfloat16 *) dev, V * ld, c->stream);
+    } else {
+        e = launch_widen_bf16((const __nv_bfloat16 *) dev, (float *) tmp, V * ld, c->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(dst_h, d * sizeof(float), tmp, ld * sizeof(float), d * sizeof(float), V,
+                                  cudaMemcpyDeviceToHost, c->stream);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    dfree(c, tmp, bytes);
+    if (e != cudaSuccess) return cuda_fail(c, e, "weights copy");
+    return PARW2V_OK;
+}
+
+int parw2v_set_weights(parw2v_ctx *c, const float *w_in, const float *w_out) {
+    if (!c) return fail(c, PARW2V_ERR_ARG, "null argument");
+    int rc = set_device(c);
+    if (!rc) rc = ensure_weights(c);
+    if (rc) return rc;
+    if (!c->weights_ready && (!w_in || !w_out))
+        return fail(c, PARW2V_ERR_STATE, "first set_weights needs both matrices (or call init_weights)");
+    if (w_in && (rc = copy_weights(c, w_in, nullptr, c->d_w_in))) return rc;
+    if (w_out && (rc = copy_weights(c, w_out, nullptr, c->d_w_out))) return rc;
+    c->weights_ready = true;
+    return PARW2V_OK;
+}
+
+int parw2v_get_weights(parw2v_ctx *c, float *w_in, float *w_out) {
+    if (!c) return fail(c, PARW2V_ERR_ARG, "null argument");
+    if (!c->weights_ready) return fail(c, PARW2V_ERR_STATE, "no weights on the device");
+    int rc = set_device(c);
+    if (rc) return rc;
+    if (w_in && (rc = copy_weights(c, nullptr, w_in, c->d_w_in))) return rc;
+    if (w_out && (rc = copy_weights(c, nullptr, w_out, c->d_w_out))) return rc;
+    return PARW2V_OK;
+}
+
+int parw2v_set_corpus(parw2v_ctx *c, const int32_t *tokens, uint64_t n) {
+    if (!c || (!tokens && n)) return fail(c, PARW2V_ERR_ARG, "null argument");
+    if (n >= 0xFFFFFFF0ULL) return fail(c, PARW2V_ERR_CAPACITY, "corpus must hold fewer than 2^32 - 16 tokens");
+    int rc = set_device(c);
+    if (rc) return rc;
+    if (n + 16 > c->corpus_cap) {
+        dfree(c, c->d_corpus, sizeof(int32_t) * c->corpus_cap);
+        c->d_corpus = nullptr;
+        c->corpus_cap = 0;
+        const uint64_t cap = n + 16;
+        if ((rc = dalloc(c, (void **) &c->d_corpus, sizeof(int32_t) * cap, "corpus"))) return rc;
+        c->corpus_cap = cap;
+    }
+    if (n) CK(c, cudaMemcpyAsync(c->d_corpus, tokens, sizeof(int32_t) * n, cudaMemcpyHostToDevice, c->stream), "corpus upload");
+    CK(c, cudaMemsetAsync(c->d_corpus + n, 0, sizeof(int32_t) * 16, c->stream), "sentinel");
+    c->n_tokens = n;
+    return PARW2V_OK;
+}
+
+int parw2v_set_trace(parw2v_ctx *c, parw2v_trace *t) {
+    if (!c) return fail(c, PARW2V_ERR_ARG, "null argument");
+    if (t && c->cfg.mode != PARW2V_MODE_DET) return fail(c, PARW2V_ERR_STATE, "traces exist in DET mode only");
+    c->trace = t;
+    return PARW2V_OK;
+}
+
+// Validation of token ids against the vocabulary (one pass, on the device).
+__global__ void k_validate(const int32_t *corpus, uint64_t n, int V, DevCounters *cnt) {
+    bool bad = false;
+    for (uint64_t i = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t) gridDim.x * blockDim.x) {
+        const int w = corpus[i];
+        bad |= (w < 0 || w >= V);
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&cnt->error, kErrCapacity);
+}
+
+static int read_counters(parw2v_ctx *c, DevCounters *h) {
+    CK(c, cudaMemcpyAsync(h, c->d_cnt, sizeof(DevCounters), cudaMemcpyDeviceToHost, c->stream), "counters");
+    CK(c, cudaStreamSynchronize(c->stream), "counters");
+    return PARW2V_OK;
+}
+
+static int device_sms(parw2v_ctx *c) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->cfg.device);
+    return sms;
+}
+
+static int train_det(parw2v_ctx *c, TrainArgs &a, parw2v_stats *st) {
+    const size_t need = (size_t) (c->cfg.batch_size + 2 * c->cfg.window * c->cfg.negative) * c->ld;
+    int rc;
+    if (c->scratch_floats < need) {
+        dfree(c, c->d_scratch, sizeof(float) * c->scratch_floats);
+        c->d_scratch = nullptr;
+        c->scratch_floats = 0;
+        if ((rc = dalloc(c, (void **) &c->d_scratch, sizeof(float) * need, "DET workspace"))) return rc;
+        c->scratch_floats = need;
+    }
+    a.scratch = c->d_scratch;
+    // trace buffers on the device
+    DevTrace dt;
+    parw2v_trace *t = c->trace;
+    void *tm = nullptr;
+    size_t tb = 0;
+    if (t) {
+        tb = (size_t) (t->keep ? t->keep_cap : 0) + (size_t) (t->b ? t->b_cap : 0) + (size_t) (t->rep_b ? t->rep_b_cap : 0) +
+             16 * 4 + sizeof(float) * (size_t) (t->alpha ? t->alpha_cap : 0) +
+             sizeof(int32_t) * (size_t) (t->neg ? t->neg_cap : 0);
+        if ((rc = dalloc(c, &tm, tb, "trace buffers"))) return rc;
+        unsigned char *p = (unsigned char *) tm;
+        auto take = [&](size_t bytes) {
+            unsigned char *q = p;
+            p += (bytes + 15) & ~(size_t) 15;
+            return q;
+        };
+        if (t->alpha) { dt.alpha = (float *) take(sizeof(float) * t->alpha_cap); dt.alpha_cap = t->alpha_cap; }
+        if (t->neg) { dt.neg = (int32_t *) take(sizeof(int32_t) * t->neg_cap); dt.neg_cap = t->neg_cap; }
+        if (t->keep) { dt.keep = (uint8_t *) take(t->keep_cap); dt.keep_cap = t->keep_cap; }
+        if (t->b) { dt.b = (uint8_t *) take(t->b_cap); dt.b_cap = t->b_cap; }
+        if (t->rep_b) { dt.rep_b = (uint8_t *) take(t->rep_b_cap); dt.rep_b_cap = t->rep_b_cap; }
+    }
+    cudaError_t e = cudaEventRecord(c->ev0, c->stream);
+    size_t smem = 0;
+    if (e == cudaSuccess) e = launch_det_train(a, dt, c->stream, &smem);
+    if (e == cudaSuccess) e = cudaEventRecord(c->ev1, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+        dfree(c, tm, tb);
+        if (smem > 200 * 1024) return fail(c, PARW2V_ERR_CAPACITY, "DET mode: window*negative*batch too large");
+        return cuda_fail(c, e, "DET training kernel");
+    }
+    DevCounters h;
+    if ((rc = read_counters(c, &h))) {
+        dfree(c, tm, tb);
+        return rc;
+    }
+    if (t) {
+        auto back = [&](void *dst, const void *src, int64_t n, size_t el) -> cudaError_t {
+            if (!dst || !src || n <= 0) return cudaSuccess;
+            return cudaMemcpy(dst, src, (size_t) n * el, cudaMemcpyDeviceToHost);
+        };
+        t->n_keep = (int64_t) h.n_keep;
+        t->n_b = (int64_t) h.n_b;
+        t->n_alpha = (int64_t) h.n_alpha;
+        t->n_rep_b = (int64_t) h.n_rep_b;
+        t->n_neg = (int64_t) h.n_neg;
+        t->final_lcg = h.final_lcg;
+        e = back(t->keep, dt.keep, std::min<int64_t>(t->n_keep, t->keep_cap), 1);
+        if (e == cudaSuccess) e = back(t->b, dt.b, std::min<int64_t>(t->n_b, t->b_cap), 1);
+        if (e == cudaSuccess) e = back(t->alpha, dt.alpha, std::min<int64_t>(t->n_alpha, t->alpha_cap), sizeof(float));
+        if (e == cudaSuccess) e = back(t->rep_b, dt.rep_b, std::min<int64_t>(t->n_rep_b, t->rep_b_cap), 1);
+        if (e == cudaSuccess) e = back(t->neg, dt.neg, std::min<int64_t>(t->n_neg, t->neg_cap), sizeof(int32_t));
+        dfree(c, tm, tb);
+        if (e != cudaSuccess) return cuda_fail(c, e, "trace download");
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    if (st) {
+        st->words = h.words;
+        st->kept = h.kept;
+        st->sentences = h.sentences;
+        st->pairs = h.pairs;
+        st->batches = h.batches;
+        st->negatives = h.negatives;
+        st->kernel_ms = ms;
+        st->pack_ms = 0;
+        st->final_alpha = h.final_alpha;
+    }
+    if (h.error & kErrResample)
+        return fail(c, PARW2V_ERR_TIMEOUT, "negative resampling exceeded its draw limit (every word is in the sentence?)");
+    return PARW2V_OK;
+}
+
+static int ensure_packing(parw2v_ctx *c) {
+    int rc;
+    const uint64_t tiles = pack_tiles(c->n_tokens) + 1;
+    if (c->corpus_cap > 0 && (!c->d_packed || c->line_cap < c->n_tokens + 1)) {
+        dfree(c, c->d_packed, sizeof(int32_t) * c->line_cap);
+        dfree(c, c->d_line_end, sizeof(uint32_t) * c->line_cap);
+        c->d_packed = nullptr;
+        c->d_line_end = nullptr;
+        const uint64_t cap = c->n_tokens + 1;
+        if ((rc = dalloc(c, (void **) &c->d_packed, sizeof(int32_t) * cap, "packed corpus"))) return rc;
+        if ((rc = dalloc(c, (void **) &c->d_line_end, sizeof(uint32_t) * cap, "line offsets"))) return rc;
+        c->line_cap = cap;
+    }
+    if (tiles > c->tile_cap) {
+        dfree(c, c->d_tile_kept, sizeof(uint32_t) * c->tile_cap);
+        dfree(c, c->d_tile_zero, sizeof(uint32_t) * c->tile_cap);
+        c->d_tile_kept = c->d_tile_zero = nullptr;
+        c->tile_cap = 0;
+        if ((rc = dalloc(c, (void **) &c->d_tile_kept, sizeof(uint32_t) * tiles, "tile sums"))) return rc;
+        if ((rc = dalloc(c, (void **) &c->d_tile_zero, sizeof(uint32_t) * tiles, "tile sums"))) return rc;
+        c->tile_cap = tiles;
+    }
+    return PARW2V_OK;
+}
+
+static int train_hogwild(parw2v_ctx *c, TrainArgs &a, parw2v_stats *st) {
+    int rc = ensure_packing(c);
+    if (rc) return rc;
+    const int sms = device_sms(c);
+    int grid = c->cfg.grid;
+    int warps = c->cfg.warps_per_cta;
+    const bool plain = c->cfg.mode == PARW2V_MODE_PLAIN;
+    if (plain) {
+        warps = plain_warps_per_cta();
+        if (!grid) grid = sms * 2;
+        const size_t per = plain_scratch_floats(c->ld, c->cfg.batch_size, c->cfg.window, c->cfg.negative);
+        const size_t need = per * (size_t) grid * warps;
+        if (c->scratch_floats < need) {
+            dfree(c, c->d_scratch, sizeof(float) * c->scratch_floats);
+            c->d_scratch = nullptr;
+            c->scratch_floats = 0;
+            if ((rc = dalloc(c, (void **) &c->d_scratch, sizeof(float) * need, "PLAIN workspace"))) return rc;
+            c->scratch_floats = need;
+        }
+        a.scratch = c->d_scratch;
+        a.scratch_per_warp = per;
+    } else {
+        size_t per_warp = 0;
+        const int maxw = batched_max_warps(c->ld, c->cfg.window, c->cfg.negative, c->cfg.batch_size, c->bf16, &per_warp);
+        if (maxw <= 0) return fail(c, PARW2V_ERR_CAPACITY, "BATCHED mode: rows do not fit in shared memory");
+        if (!warps || warps > maxw) warps = maxw;
+        if (!grid) grid = sms;
+    }
+    float pack_ms_total = 0.f, kernel_ms_total = 0.f;
+    for (int ep = 0; ep < c->cfg.iter; ep++) {
+        a.epoch = ep;
+        CK(c, cudaMemsetAsync(&c->d_cnt->work, 0, sizeof(unsigned long long), c->stream), "counters");
+        CK(c, cudaEventRecord(c->ev0, c->stream), "event");
+        CK(c, launch_pack(a, c->d_packed, c->d_line_end, c->d_tile_kept, c->d_tile_zero, pack_tiles(c->n_tokens), c->stream),
+           "packing kernels");
+        CK(c, cudaEventRecord(c->ev1, c->stream), "event");
+        cudaError_t e = plain ? launch_plain_train(a, grid, warps, c->stream)
+                              : launch_batched_train(a, c->bf16, grid, warps, c->stream);
+        if (e != cudaSuccess) return cuda_fail(c, e, "training kernel launch");
+        CK(c, cudaEventRecord(c->ev2, c->stream), "event");
+        CK(c, cudaStreamSynchronize(c->stream), "training kernel");
+        float m0 = 0, m1 = 0;
+        cudaEventElapsedTime(&m0, c->ev0, c->ev1);
+        cudaEventElapsedTime(&m1, c->ev1, c->ev2);
+        pack_ms_total += m0;
+        kernel_ms_total += m1;
+    }
+    DevCounters h;
+    if ((rc = read_counters(c, &h))) return rc;
+    if (st) {
+        st->words = (uint64_t) c->n_tokens * (uint64_t) c->cfg.iter;
+        st->kept = h.kept;
+        st->sentences = h.sentences;
+        st->pairs = h.pairs;
+        st->batches = h.batches;
+        st->negatives = h.negatives;
+        st->kernel_ms = kernel_ms_total;
+        st->pack_ms = pack_ms_total;
+        st->final_alpha = c->cfg.alpha * 0.0001f;
+    }
+    if (h.error & kErrResample)
+        return fail(c, PARW2V_ERR_TIMEOUT, "negative resampling exceeded its draw limit (every word is in the sentence?)");
+    return PARW2V_OK;
+}
+
+int parw2v_train(parw2v_ctx *c, parw2v_stats *st) {
+    if (!c) return fail(c, PARW2V_ERR_ARG, "null argument");
+    if (!c->vocab) return fail(c, PARW2V_ERR_STATE, "set_vocab first");
+    if (!c->weights_ready) return fail(c, PARW2V_ERR_STATE, "init_weights or set_weights first");
+    if (!c->d_corpus) return fail(c, PARW2V_ERR_STATE, "set_corpus first");
+    if (st) memset(st, 0, sizeof(*st));
+    int rc = set_device(c);
+    if (rc) return rc;
+    CK(c, cudaMemsetAsync(c->d_cnt, 0, sizeof(DevCounters), c->stream), "counters");
+    if (c->n_tokens) {
+        k_validate<<<148 * 4, 256, 0, c->stream>>>(c->d_corpus, c->n_tokens, c->vocab, c->d_cnt);
+        CK(c, cudaGetLastError(), "validation kernel");
+    }
+    DevCounters h;
+    if ((rc = read_counters(c, &h))) return rc;
+    if (h.error & kErrCapacity) return fail(c, PARW2V_ERR_ARG, "corpus holds ids outside [0, vocab_size)");
+    TrainArgs a{};
+    a.corpus = c->d_corpus;
+    a.n_tokens = c->n_tokens;
+    a.keep_thr = c->d_thr;
+    a.table = c->d_table;
+    a.exp_table = c->d_exp;
+    a.w_in = c->d_w_in;
+    a.w_out = c->d_w_out;
+    a.ld = c->ld;
+    a.d = c->cfg.size;
+    a.window = c->cfg.window;
+    a.negative = c->cfg.negative;
+    a.batch = c->cfg.batch_size;
+    a.iter = c->cfg.iter;
+    a.vocab = c->vocab;
+    a.alpha0 = c->cfg.alpha;
+    a.sample = c->cfg.sample;
+    a.train_words = c->train_words;
+    a.seed = c->cfg.seed;
+    a.cnt = c->d_cnt;
+    a.packed = c->d_packed;
+    a.line_end = c->d_line_end;
+    a.max_resample = 1LL << 20;
+    if (c->cfg.mode == PARW2V_MODE_DET) return train_det(c, a, st);
+    rc = ensure_packing(c);
+    if (rc) return rc;
+    a.packed = c->d_packed;
+    a.line_end = c->d_line_end;
+    return train_hogwild(c, a, st);
+}
+
+// ---- loss / adjoint / finite differences ----
+struct DevBatch {
+    void *mem = nullptr;
+    size_t bytes = 0;
+    LossBatch b{};
+};
+
+static int upload_batch(parw2v_ctx *c, const int32_t *tgt, const int32_t *ctxw, int n_pairs, const int32_t *neg,
+                        int n_neg, int cpw, DevBatch &db) {
+    if (!tgt || !ctxw || n_pairs <= 0 || cpw <= 0 || n_neg < 0 || (n_neg > 0 && !neg))
+        return fail(c, PARW2V_ERR_ARG, "invalid minibatch");
+    if (!c->weights_ready) return fail(c, PARW2V_ERR_STATE, "no weights on the device");
+    const int n_win = (n_pairs + cpw - 1) / cpw;
+    for (int i = 0; i < n_pairs; i++)
+        if (tgt[i] < 0 || tgt[i] >= c->vocab || ctxw[i] < 0 || ctxw[i] >= c->vocab)
+            return fail(c, PARW2V_ERR_ARG, "minibatch id outside the vocabulary");
+    for (long long i = 0; i < (long long) n_win * n_neg; i++)
+        if (neg[i] < 0 || neg[i] >= c->vocab) return fail(c, PARW2V_ERR_ARG, "negative id outside the vocabulary");
+    const size_t n_negs = (size_t) n_win * n_neg;
+    db.bytes = sizeof(int32_t) * (2 * (size_t) n_pairs + n_negs + 4);
+    int rc = dalloc(c, &db.mem, db.bytes, "minibatch");
+    if (rc) return rc;
+    int32_t *p = (int32_t *) db.mem;
+    cudaError_t e = cudaMemcpyAsync(p, tgt, sizeof(int32_t) * n_pairs, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(p + n_pairs, ctxw, sizeof(int32_t) * n_pairs, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && n_negs)
+        e = cudaMemcpyAsync(p + 2 * n_pairs, neg, sizeof(int32_t) * n_negs, cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) {
+        dfree(c, db.mem, db.bytes);
+        return cuda_fail(c, e, "minibatch upload");
+    }
+    db.b.tgt = p;
+    db.b.ctx = p + n_pairs;
+    db.b.neg = p + 2 * n_pairs;
+    db.b.n_pairs = n_pairs;
+    db.b.n_neg = n_neg;
+    db.b.ctx_per_window = cpw;
+    return PARW2V_OK;
+}
+
+int parw2v_loss(parw2v_ctx *c, const int32_t *tgt, const int32_t *ctxw, int n_pairs, const int32_t *neg, int n_neg,
+                int cpw, double *loss) {
+    if (!c || !loss) return fail(c, PARW2V_ERR_ARG, "null argument");
+    int rc = set_device(c);
+    if (rc) return rc;
+    DevBatch db;
+    if ((rc = upload_batch(c, tgt, ctxw, n_pairs, neg, n_neg, cpw, db))) return rc;
+    double *d_out = nullptr;
+    if ((rc = dalloc(c, (void **) &d_out, sizeof(double), "loss"))) {
+        dfree(c, db.mem, db.bytes);
+        return rc;
+    }
+    cudaError_t e = cudaMemsetAsync(d_out, 0, sizeof(double), c->stream);
+    if (e == cudaSuccess) e = launch_loss(db.b, c->d_w_in, c->d_w_out, c->bf16, c->cfg.size, c->ld, d_out, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(loss, d_out, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    dfree(c, d_out, sizeof(double));
+    dfree(c, db.mem, db.bytes);
+    if (e != cudaSuccess) return cuda_fail(c, e, "loss kernel");
+    return PARW2V_OK;
+}
+
+int parw2v_loss_adjoint(parw2v_ctx *c, const int32_t *tgt, const int32_t *ctxw, int n_pairs, const int32_t *neg,
+                        int n_neg, int cpw, int exact, float *d_w_in, float *d_w_out) {
+    if (!c) return fail(c, PARW2V_ERR_ARG, "null argument");
+    int rc = set_device(c);
+    if (rc) return rc;
+    DevBatch db;
+    if ((rc = upload_batch(c, tgt, ctxw, n_pairs, neg, n_neg, cpw, db))) return rc;
+    const size_t V = (size_t) c->vocab, ld = (size_t) c->ld, d = (size_t) c->cfg.size;
+    const size_t bytes = sizeof(float) * V * ld * 2;
+    float *g = nullptr;
+    if ((rc = dalloc(c, (void **) &g, bytes, "gradient buffers"))) {
+        dfree(c, db.mem, db.bytes);
+        return rc;
+    }
+    cudaError_t e = cudaMemsetAsync(g, 0, bytes, c->stream);
+    if (e == cudaSuccess)
+        e = launch_adjoint(db.b, c->d_w_in, c->d_w_out, c->bf16, c->cfg.size, c->ld, c->d_exp, exact, g, g + V * ld,
+                           c->stream);
+    if (e == cudaSuccess && d_w_in)
+        e = cudaMemcpy2DAsync(d_w_in, d * sizeof(float), g, ld * sizeof(float), d * sizeof(float), V,
+                              cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess && d_w_out)
+        e = cudaMemcpy2DAsync(d_w_out, d * sizeof(float), g + V * ld, ld * sizeof(float), d * sizeof(float), V,
+                              cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    dfree(c, g, bytes);
+    dfree(c, db.mem, db.bytes);
+    if (e != cudaSuccess) return cuda_fail(c, e, "adjoint kernel");
+    return PARW2V_OK;
+}
+
+int parw2v_loss_fd(parw2v_ctx *c, const int32_t *tgt, const int32_t *ctxw, int n_pairs, const int32_t *neg, int n_neg,
+                   int cpw, const int32_t *matrix, const int32_t *row, const int32_t *col, int n_probes, double h,
+                   double *grad) {
+    if (!c || !matrix || !row || !col || !grad || n_probes <= 0 || !(h > 0)) return fail(c, PARW2V_ERR_ARG, "invalid probes");
+    for (int i = 0; i < n_probes; i++)
+        if ((matrix[i] != 0 && matrix[i] != 1) || row[i] < 0 || row[i] >= c->vocab || col[i] < 0 || col[i] >= c->cfg.size)
+            return fail(c, PARW2V_ERR_ARG, "probe outside the weights");
+    int rc = set_device(c);
+    if (rc) return rc;
+    DevBatch db;
+    if ((rc = upload_batch(c, tgt, ctxw, n_pairs, neg, n_neg, cpw, db))) return rc;
+    const size_t pb = sizeof(int32_t) * 3 * (size_t) n_probes + sizeof(double) * (size_t) n_probes + 16;
+    void *pm = nullptr;
+    if ((rc = dalloc(c, &pm, pb, "probes"))) {
+        dfree(c, db.mem, db.bytes);
+        return rc;
+    }
+    double *d_grad = (double *) pm;
+    int32_t *d_m = (int32_t *) (d_grad + n_probes);
+    cudaError_t e = cudaMemcpyAsync(d_m, matrix, sizeof(int32_t) * n_probes, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_m + n_probes, row, sizeof(int32_t) * n_probes, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_m + 2 * n_probes, col, sizeof(int32_t) * n_probes, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess)
+        e = launch_loss_fd(db.b, c->d_w_in, c->d_w_out, c->bf16, c->cfg.size, c->ld, d_m, d_m + n_probes,
+                           d_m + 2 * n_probes, n_probes, h, d_grad, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(grad, d_grad, sizeof(double) * n_probes, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    dfree(c, pm, pb);
+    dfree(c, db.mem, db.bytes);
+    if (e != cudaSuccess) return cuda_fail(c, e, "finite-difference kernel");
+    return PARW2V_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,75 @@
+// Device helpers shared by the PAR-Word2Vec kernels (sm_100a).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+
+namespace parw2v {
+
+constexpr int kTableSize = 100000000;  // unigram table entries, PAR_Word2Vec_cpu.cpp:75
+constexpr int kExpTableSize = 1000;    // PAR_Word2Vec_cpu.cpp:32
+constexpr int kMaxExp = 6;             // PAR_Word2Vec_cpu.cpp:33
+constexpr int kMaxSentence = 1000;     // PAR_Word2Vec_cpu.cpp:34
+// EXP_TABLE_SIZE / (MAX_EXP * 2.0f) rounded to float, PAR_Word2Vec_cpu.cpp:70
+constexpr float kExpResolution = 1000.0f / 12.0f;
+
+// Error bits raised by kernels into the context's device status word.
+constexpr unsigned kErrResample = 1u;  // a negative-resampling loop hit its draw limit
+constexpr unsigned kErrCapacity = 2u;  // an input exceeded a kernel's fixed capacity
+
+// The reference's linear congruential generator, next = next * 25214903917 + 11 (mod 2^64),
+// PAR_Word2Vec_cpu.cpp:461, :532, :591-612.
+__host__ __device__ __forceinline__ uint64_t lcg_next(uint64_t x) {
+    return x * 25214903917ULL + 11ULL;
+}
+
+// Affine map x -> a*x + c (mod 2^64); composing n LCG steps gives a jump-ahead in O(log n).
+struct Affine {
+    uint64_t a, c;
+};
+__host__ __device__ __forceinline__ Affine affine_then(Affine first, Affine second) {
+    return Affine{second.a * first.a, second.a * first.c + second.c};
+}
+__host__ __device__ inline uint64_t lcg_jump(uint64_t x, uint64_t n) {
+    Affine acc{1ULL, 0ULL}, step{25214903917ULL, 11ULL};
+    while (n) {
+        if (n & 1ULL) acc = affine_then(acc, step);
+        step = affine_then(step, step);
+        n >>= 1;
+    }
+    return acc.a * x + acc.c;
+}
+
+// SplitMix64 finaliser (Steele, Lea & Flood 2014): a bijective 64-bit mixer used to derive
+// independent per-token / per-sentence random streams in the Hogwild modes.
+__host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+// g = (label - sigma(f)) * alpha through the clamped expTable (PAR_Word2Vec_cpu.cpp:554-559 for
+// label 1, :642-647 for label 0).  Explicit round-to-nearest intrinsics keep every operation a
+// single IEEE rounding, as in the reference built without contraction.  The index is clamped
+// into the table, which only matters for a NaN dot product (undefined in the reference).
+__device__ __forceinline__ float grad_from_table(float f, int label, float alpha, const float *exp_table) {
+    if (f > (float) kMaxExp) return __fmul_rn((float) (label - 1), alpha);
+    if (f < -(float) kMaxExp) return __fmul_rn((float) label, alpha);
+    int idx = __float2int_rz(__fmul_rn(__fadd_rn(f, (float) kMaxExp), kExpResolution));
+    idx = idx < 0 ? 0 : (idx > kExpTableSize ? kExpTableSize : idx);
+    return __fmul_rn(__fsub_rn((float) label, exp_table[idx]), alpha);
+}
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Fire-and-forget vector reduction into global memory (sm_90+): one L2 atomic per 8 bytes.
+__device__ __forceinline__ void red_add_f2(float *addr, float2 v) {
+    asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(addr), "f"(v.x), "f"(v.y) : "memory");
+}
+
+}  // namespace parw2v

@@ -1,0 +1,284 @@
+// PLAIN mode: FP32 Hogwild, one warp per sentence, every row read from and written to global
+// memory at each use.  This is the straightforward GPU formulation of PAR_Word2Vec_cpu's thread
+// loop (PAR_Word2Vec_cpu.cpp:529-679) and the baseline the data-local kernel is measured against.
+//
+// Per sentence (a "</s>"-terminated line of the packed corpus, cut every 1000 kept tokens):
+//   attraction  for each position: b from the sentence's LCG; the target's W_out row lives in
+//               registers (lane l owns float2 chunks l, l+32, ...); each context's W_in row is
+//               loaded, dotted (warp shuffle reduction), updated and stored back;
+//   repulsion   per batch of `batch` positions: rep_b and rep_b * negative shared negatives from
+//               the unigram table, redrawn uniformly while they occur in the sentence; M_in and
+//               M_out are staged in the warp's global workspace, the three products run on the
+//               warp, and the updates are added with vector red.global.add.
+// Random streams: the sentence's LCG starts from mix64(seed, epoch, line, piece); the learning
+// rate decays linearly with the sentence's position in the corpus (the reference decays with the
+// words processed so far, :443).
+#include "common.cuh"
+#include "internal.h"
+
+namespace parw2v {
+
+namespace {
+
+constexpr int kPlainWarps = 8;
+
+template <int NV2>
+struct RowReg {
+    float2 v[NV2];
+};
+
+template <int NV2>
+__device__ __forceinline__ void load_row(RowReg<NV2> &r, const float *row, int n2, int lane) {
+    const float2 *p = reinterpret_cast<const float2 *>(row);
+#pragma unroll
+    for (int i = 0; i < NV2; i++) {
+        const int q = lane + 32 * i;
+        r.v[i] = q < n2 ? p[q] : make_float2(0.f, 0.f);
+    }
+}
+template <int NV2>
+__device__ __forceinline__ void store_row(const RowReg<NV2> &r, float *row, int n2, int lane) {
+    float2 *p = reinterpret_cast<float2 *>(row);
+#pragma unroll
+    for (int i = 0; i < NV2; i++) {
+        const int q = lane + 32 * i;
+        if (q < n2) p[q] = r.v[i];
+    }
+}
+template <int NV2>
+__device__ __forceinline__ float dot_row(const RowReg<NV2> &a, const RowReg<NV2> &b) {
+    float s = 0.f;
+#pragma unroll
+    for (int i = 0; i < NV2; i++) s = fmaf(a.v[i].x, b.v[i].x, fmaf(a.v[i].y, b.v[i].y, s));
+    return warp_sum(s);
+}
+
+__device__ __forceinline__ float sentence_alpha(const TrainArgs &a, uint64_t kept_before, uint64_t total_kept) {
+    // words processed so far, as the fraction of this epoch's kept tokens before the sentence
+    const double done = (double) a.epoch * (double) a.n_tokens +
+                        (total_kept ? (double) kept_before / (double) total_kept : 0.0) * (double) a.n_tokens;
+    float alpha = a.alpha0 * (float) (1.0 - done / ((double) a.iter * (double) a.train_words + 1.0));
+    const float floor_a = a.alpha0 * 0.0001f;
+    return alpha < floor_a ? floor_a : alpha;
+}
+
+__device__ __forceinline__ uint64_t sentence_seed(const TrainArgs &a, uint64_t line, int piece) {
+    return mix64(mix64(a.seed ^ (0xD1B54A32D192ED03ULL * (uint64_t) (a.epoch + 1))) ^ (line * 1024ULL + piece));
+}
+
+// Shared negative draw (PAR_Word2Vec_cpu.cpp:603-622) with the membership test spread over the warp.
+__device__ __forceinline__ int draw_negative(const TrainArgs &a, uint64_t &rng, const int *sen, int len, int lane,
+                                             bool &failed) {
+    rng = lcg_next(rng);
+    int s = __ldg(a.table + (rng >> 16) % (uint64_t) kTableSize);
+    if (!s) s = (int) (rng % (uint64_t) (a.vocab - 1) + 1);
+    for (int64_t tries = 0;; tries++) {
+        bool hit = false;
+        for (int q = lane; q < len; q += 32) hit |= (sen[q] == s);
+        if (!__any_sync(0xffffffffu, hit)) break;
+        if (tries >= a.max_resample) {
+            failed = true;
+            break;
+        }
+        rng = lcg_next(rng);
+        s = (int) (rng % (uint64_t) (a.vocab - 1) + 1);
+    }
+    return s;
+}
+
+template <int NV2>
+__global__ void __launch_bounds__(kPlainWarps * 32) k_plain_train(TrainArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int w = a.window, B = a.batch, ld = a.ld;
+    const int n2 = (a.d + 1) >> 1;
+    const int kmax = 2 * w * a.negative;
+    float *s_exp = reinterpret_cast<float *>(smem_raw);  // 1004
+    unsigned char *warp_base = smem_raw + 1004 * sizeof(float) +
+                               (size_t) wid * (sizeof(int) * (kMaxSentence + kmax) + sizeof(float) * kmax * B);
+    int *sen = reinterpret_cast<int *>(warp_base);
+    int *negs = sen + kMaxSentence;
+    float *grad = reinterpret_cast<float *>(negs + kmax);
+    for (int i = threadIdx.x; i <= kExpTableSize; i += blockDim.x) s_exp[i] = a.exp_table[i];
+    __syncthreads();
+
+    float *w_in = static_cast<float *>(a.w_in);
+    float *w_out = static_cast<float *>(a.w_out);
+    const size_t gwarp = (size_t) blockIdx.x * kPlainWarps + wid;
+    float *m_in = a.scratch + gwarp * a.scratch_per_warp;  // B x ld
+    float *m_out = m_in + (size_t) B * ld;                  // kmax x ld
+    const uint64_t n_lines = a.cnt->n_lines, total_kept = a.cnt->total_kept;
+    unsigned long long st_kept = 0, st_sent = 0, st_pairs = 0, st_batches = 0, st_negs = 0;
+    bool failed = false;
+
+    for (;;) {
+        unsigned long long line = 0;
+        if (lane == 0) line = atomicAdd(&a.cnt->work, 1ULL);
+        line = __shfl_sync(0xffffffffu, line, 0);
+        if (line >= n_lines || failed) break;
+        const uint32_t lo = line ? a.line_end[line - 1] : 0u, hi = a.line_end[line];
+        int piece = 0;
+        for (uint32_t c0 = lo; c0 < hi; c0 += kMaxSentence, piece++) {
+            const int L = (int) min((uint32_t) kMaxSentence, hi - c0);
+            for (int i = lane; i < L; i += 32) sen[i] = a.packed[c0 + i];
+            __syncwarp();
+            uint64_t rng = sentence_seed(a, line, piece);
+            const float alpha = sentence_alpha(a, c0, total_kept);
+
+            // ---- attraction (:529-568) ----
+            for (int pos = 0; pos < L; pos++) {
+                rng = lcg_next(rng);
+                const int b = (int) (rng % (uint64_t) w);
+                float *y = w_out + (size_t) sen[pos] * ld;
+                RowReg<NV2> yr;
+                load_row(yr, y, n2, lane);
+                for (int i = b; i < 2 * w + 1 - b; i++) {
+                    if (i == w) continue;
+                    const int c = pos - w + i;
+                    if (c < 0) continue;
+                    if (c >= L) break;
+                    float *x = w_in + (size_t) sen[c] * ld;
+                    RowReg<NV2> xr;
+                    load_row(xr, x, n2, lane);
+                    const float g = grad_from_table(dot_row(xr, yr), 1, alpha, s_exp);
+#pragma unroll
+                    for (int q = 0; q < NV2; q++) {
+                        const float2 xv = xr.v[q], yv = yr.v[q];
+                        xr.v[q] = make_float2(fmaf(g, yv.x, xv.x), fmaf(g, yv.y, xv.y));
+                        yr.v[q] = make_float2(fmaf(g, xv.x, yv.x), fmaf(g, xv.y, yv.y));
+                    }
+                    store_row(xr, x, n2, lane);
+                    st_pairs++;
+                }
+                store_row(yr, y, n2, lane);
+            }
+
+            // ---- repulsion (:571-679) ----
+            const int num_batch = (L + B - 1) / B;
+            for (int nb = 0; nb < num_batch && !failed; nb++) {
+                const int lo_b = nb * B;
+                const int rows = min(B, L - lo_b);
+                rng = lcg_next(rng);
+                const int rep_b = (lo_b <= w - 1 || (L - 1) - lo_b <= w - 1) ? (int) (rng % (uint64_t) w)
+                                                                              : (int) (rng % (uint64_t) (2 * w));
+                const int K = rep_b * a.negative;
+                for (int k = 0; k < K; k++) {
+                    const int s = draw_negative(a, rng, sen, L, lane, failed);
+                    if (lane == 0) negs[k] = s;
+                }
+                st_batches++;
+                st_negs += K;
+                __syncwarp();
+                // stage pre-update copies of the batch rows and the negatives' rows
+                for (int r = 0; r < rows; r++) {
+                    RowReg<NV2> t;
+                    load_row(t, w_in + (size_t) sen[lo_b + r] * ld, n2, lane);
+                    store_row(t, m_in + (size_t) r * ld, n2, lane);
+                }
+                for (int k = 0; k < K; k++) {
+                    RowReg<NV2> t;
+                    load_row(t, w_out + (size_t) negs[k] * ld, n2, lane);
+                    store_row(t, m_out + (size_t) k * ld, n2, lane);
+                }
+                __syncwarp();
+                // MM1 + sigma / label 0
+                for (int k = 0; k < K; k++) {
+                    RowReg<NV2> o;
+                    load_row(o, m_out + (size_t) k * ld, n2, lane);
+                    for (int r = 0; r < rows; r++) {
+                        RowReg<NV2> in;
+                        load_row(in, m_in + (size_t) r * ld, n2, lane);
+                        const float f = dot_row(o, in);
+                        if (lane == 0) grad[k * rows + r] = grad_from_table(f, 0, alpha, s_exp);
+                    }
+                }
+                __syncwarp();
+                // MM2: W_out[neg_k] += sum_r grad[k][r] M_in[r]
+                for (int k = 0; k < K; k++) {
+                    RowReg<NV2> acc;
+#pragma unroll
+                    for (int q = 0; q < NV2; q++) acc.v[q] = make_float2(0.f, 0.f);
+                    for (int r = 0; r < rows; r++) {
+                        RowReg<NV2> in;
+                        load_row(in, m_in + (size_t) r * ld, n2, lane);
+                        const float g = grad[k * rows + r];
+#pragma unroll
+                        for (int q = 0; q < NV2; q++)
+                            acc.v[q] = make_float2(fmaf(g, in.v[q].x, acc.v[q].x), fmaf(g, in.v[q].y, acc.v[q].y));
+                    }
+                    float *dst = w_out + (size_t) negs[k] * ld;
+#pragma unroll
+                    for (int q = 0; q < NV2; q++)
+                        if (lane + 32 * q < n2) red_add_f2(dst + 2 * (lane + 32 * q), acc.v[q]);
+                }
+                // MM3: W_in[sen[lo_b + r]] += sum_k grad[k][r] M_out[k]
+                for (int r = 0; r < rows; r++) {
+                    RowReg<NV2> acc;
+#pragma unroll
+                    for (int q = 0; q < NV2; q++) acc.v[q] = make_float2(0.f, 0.f);
+                    for (int k = 0; k < K; k++) {
+                        RowReg<NV2> o;
+                        load_row(o, m_out + (size_t) k * ld, n2, lane);
+                        const float g = grad[k * rows + r];
+#pragma unroll
+                        for (int q = 0; q < NV2; q++)
+                            acc.v[q] = make_float2(fmaf(g, o.v[q].x, acc.v[q].x), fmaf(g, o.v[q].y, acc.v[q].y));
+                    }
+                    float *dst = w_in + (size_t) sen[lo_b + r] * ld;
+#pragma unroll
+                    for (int q = 0; q < NV2; q++)
+                        if (lane + 32 * q < n2) red_add_f2(dst + 2 * (lane + 32 * q), acc.v[q]);
+                }
+                __syncwarp();
+            }
+            st_kept += L;
+            st_sent++;
+            __syncwarp();
+        }
+    }
+    if (lane == 0) {
+        atomicAdd(&a.cnt->kept, st_kept);
+        atomicAdd(&a.cnt->sentences, st_sent);
+        atomicAdd(&a.cnt->pairs, st_pairs);
+        atomicAdd(&a.cnt->batches, st_batches);
+        atomicAdd(&a.cnt->negatives, st_negs);
+        if (failed) atomicOr(&a.cnt->error, kErrResample);
+    }
+}
+
+template <int NV2>
+cudaError_t launch_plain_nv(const TrainArgs &a, int grid, int warps, cudaStream_t s) {
+    (void) warps;
+    const int kmax = 2 * a.window * a.negative;
+    const size_t smem = 1004 * sizeof(float) +
+                        (size_t) kPlainWarps * (sizeof(int) * (kMaxSentence + kmax) + sizeof(float) * kmax * a.batch);
+    cudaError_t e = cudaFuncSetAttribute(k_plain_train<NV2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    if (e != cudaSuccess) return e;
+    k_plain_train<NV2><<<grid, kPlainWarps * 32, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t plain_scratch_floats(int ld, int batch, int window, int negative) {
+    return (size_t) (batch + 2 * window * negative) * ld;
+}
+
+int plain_warps_per_cta() { return kPlainWarps; }
+
+cudaError_t launch_plain_train(const TrainArgs &a, int grid, int warps_per_cta, cudaStream_t s) {
+    const int nv2 = (a.d + 63) / 64;
+    switch (nv2) {
+        case 1: return launch_plain_nv<1>(a, grid, warps_per_cta, s);
+        case 2: return launch_plain_nv<2>(a, grid, warps_per_cta, s);
+        case 3: return launch_plain_nv<3>(a, grid, warps_per_cta, s);
+        case 4: return launch_plain_nv<4>(a, grid, warps_per_cta, s);
+        case 5: return launch_plain_nv<5>(a, grid, warps_per_cta, s);
+        case 6: return launch_plain_nv<6>(a, grid, warps_per_cta, s);
+        case 7: return launch_plain_nv<7>(a, grid, warps_per_cta, s);
+        case 8: return launch_plain_nv<8>(a, grid, warps_per_cta, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace parw2v

@@ -1,0 +1,163 @@
+// Set-up kernels: subsampling thresholds, the unigram^0.75 table, InitNet, BF16 conversions.
+#include "common.cuh"
+#include "internal.h"
+
+namespace parw2v {
+
+// keep_thr[w] = sqrtf(ratio) + ratio, ratio = (sample * (float) train_words) / (float) cn[w]
+// (PAR_Word2Vec_cpu.cpp:459-460).  A token is dropped when keep_thr < (rand & 0xFFFF) / 65536.
+__global__ void k_thresholds(const uint32_t *cn, int V, float sample, uint64_t train_words, float *thr) {
+    int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= V) return;
+    float ratio = __fdiv_rn(__fmul_rn(sample, __ull2float_rn(train_words)), __uint2float_rn(cn[w]));
+    thr[w] = __fadd_rn(__fsqrt_rn(ratio), ratio);
+}
+
+cudaError_t launch_build_thresholds(const uint32_t *counts, int V, float sample, uint64_t train_words,
+                                    float *keep_thr, cudaStream_t s) {
+    k_thresholds<<<(V + 255) / 256, 256, 0, s>>>(counts, V, sample, train_words, keep_thr);
+    return cudaGetLastError();
+}
+
+// ---- unigram table (PAR_Word2Vec_cpu.cpp:96-117) ----
+// The reference fills the table sequentially: slot a gets the current word i, then i advances
+// when a / 1e8f > d1, where d1 is a float running sum of the double quotients cn^0.75 / total.
+// Word i therefore owns slots [t_i, e_i] with e_i = max(t_i, g_i), g_i the first slot whose
+// float position exceeds threshold D_i, and t_{i+1} = e_i + 1.  The two V-long recurrences
+// (the FP64 total with the float running sum, and the max-plus start recurrence) run on one
+// thread each, exactly as ordered in the reference; the 27-step threshold search per word and
+// the 1e8-slot fill run in parallel.
+
+// One thread: total = sum of pow_cn in index order (the reference's reduction at one thread),
+// then D_i (float), the value of d1 while word i is current.
+__global__ void k_table_thresholds(const double *pow_cn, int V, float *D, double *total_out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double total = 0.0;
+    for (int i = 0; i < V; i++) total += pow_cn[i];
+    *total_out = total;
+    float d1 = (float) (pow_cn[0] / total);
+    D[0] = d1;
+    for (int i = 1; i < V; i++) {
+        d1 = (float) ((double) d1 + pow_cn[i] / total);
+        D[i] = d1;
+    }
+}
+
+__device__ __forceinline__ float slot_position(int a) {  // a / (real) table_size
+    return __fdiv_rn(__int2float_rn(a), (float) kTableSize);
+}
+
+// g_i = first slot a in [0, 1e8) with a / 1e8f > D_i, or 1e8 when there is none.
+__global__ void k_table_first_slot(const float *D, int V, long long *g) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= V) return;
+    const float x = D[i];
+    int lo = 0, hi = kTableSize;
+    while (lo < hi) {
+        int mid = lo + ((hi - lo) >> 1);
+        if (slot_position(mid) > x) hi = mid;
+        else lo = mid + 1;
+    }
+    g[i] = lo;
+}
+
+// One thread: t_0 = 0, t_{i+1} = max(t_i, g_i) + 1, written in place over g.
+__global__ void k_table_starts(long long *g_then_t, int V) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    long long t = 0;
+    for (int i = 0; i < V; i++) {
+        long long gi = g_then_t[i];
+        g_then_t[i] = t;
+        t = (t > gi ? t : gi) + 1;
+    }
+}
+
+// Fill: slot a holds the last word i with t_i <= a (word V-1 from t_{V-1} on: the clamp).
+constexpr int kFillChunk = 1024;
+__global__ void k_table_fill(const long long *t, int V, int32_t *table) {
+    long long a0 = ((long long) blockIdx.x * blockDim.x + threadIdx.x) * kFillChunk;
+    if (a0 >= kTableSize) return;
+    int lo = 0, hi = V - 1;  // largest i with t_i <= a0 (t_0 = 0 <= a0)
+    while (lo < hi) {
+        int mid = lo + ((hi - lo + 1) >> 1);
+        if (t[mid] <= a0) lo = mid;
+        else hi = mid - 1;
+    }
+    int i = lo;
+    long long a1 = a0 + kFillChunk < kTableSize ? a0 + kFillChunk : kTableSize;
+    long long next = (i + 1 < V) ? t[i + 1] : (1LL << 62);
+    for (long long a = a0; a < a1; a++) {
+        while (a >= next) {
+            i++;
+            next = (i + 1 < V) ? t[i + 1] : (1LL << 62);
+        }
+        table[a] = i;
+    }
+}
+
+cudaError_t launch_build_table(const double *pow_cn, int V, int32_t *table, float *D, long long *g,
+                               double *total, cudaStream_t s) {
+    k_table_thresholds<<<1, 32, 0, s>>>(pow_cn, V, D, total);
+    k_table_first_slot<<<(V + 255) / 256, 256, 0, s>>>(D, V, g);
+    k_table_starts<<<1, 32, 0, s>>>(g, V);
+    const long long chunks = (kTableSize + kFillChunk - 1) / kFillChunk;
+    k_table_fill<<<(unsigned) ((chunks + 255) / 256), 256, 0, s>>>(g, V, table);
+    return cudaGetLastError();
+}
+
+// ---- InitNet (PAR_Word2Vec_cpu.cpp:337-357) ----
+// Element i (row-major over [V][d]) takes the LCG state after i + 1 steps from seed 1; each
+// thread jumps to the start of its chunk in O(log i) and then steps sequentially.
+constexpr int kInitChunk = 256;
+__global__ void k_init_net(float *w_in, __nv_bfloat16 *b_in, int V, int d, int ld) {
+    const long long n = (long long) V * d;
+    const long long s0 = ((long long) blockIdx.x * blockDim.x + threadIdx.x) * kInitChunk;
+    if (s0 >= n) return;
+    uint64_t r = lcg_jump(1ULL, (uint64_t) s0);
+    const long long s1 = s0 + kInitChunk < n ? s0 + kInitChunk : n;
+    const float fd = (float) d;
+    for (long long i = s0; i < s1; i++) {
+        r = lcg_next(r);
+        float v = __fdiv_rn(__fsub_rn(__fdiv_rn((float) (r & 0xFFFF), 65536.f), 0.5f), fd);
+        long long row = i / d, col = i - row * d;
+        if (w_in) w_in[row * ld + col] = v;
+        else b_in[row * ld + col] = __float2bfloat16_rn(v);
+    }
+}
+
+cudaError_t launch_init_net(float *w_in, float *w_out, __nv_bfloat16 *b_in, __nv_bfloat16 *b_out, int V, int d,
+                            int ld, cudaStream_t s) {
+    const size_t elems = (size_t) V * ld;
+    cudaError_t e;
+    if (w_in) {
+        if ((e = cudaMemsetAsync(w_in, 0, elems * sizeof(float), s)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(w_out, 0, elems * sizeof(float), s)) != cudaSuccess) return e;
+    } else {
+        if ((e = cudaMemsetAsync(b_in, 0, elems * sizeof(__nv_bfloat16), s)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(b_out, 0, elems * sizeof(__nv_bfloat16), s)) != cudaSuccess) return e;
+    }
+    const long long n = (long long) V * d;
+    const long long threads = (n + kInitChunk - 1) / kInitChunk;
+    k_init_net<<<(unsigned) ((threads + 255) / 256), 256, 0, s>>>(w_in, b_in, V, d, ld);
+    return cudaGetLastError();
+}
+
+// ---- BF16 <-> FP32 ----
+__global__ void k_widen(const __nv_bfloat16 *src, float *dst, size_t n) {
+    for (size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t) gridDim.x * blockDim.x)
+        dst[i] = __bfloat162float(src[i]);
+}
+__global__ void k_narrow(const float *src, __nv_bfloat16 *dst, size_t n) {
+    for (size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t) gridDim.x * blockDim.x)
+        dst[i] = __float2bfloat16_rn(src[i]);
+}
+cudaError_t launch_widen_bf16(const __nv_bfloat16 *src, float *dst, size_t n, cudaStream_t s) {
+    k_widen<<<148 * 8, 256, 0, s>>>(src, dst, n);
+    return cudaGetLastError();
+}
+cudaError_t launch_narrow_bf16(const float *src, __nv_bfloat16 *dst, size_t n, cudaStream_t s) {
+    k_narrow<<<148 * 8, 256, 0, s>>>(src, dst, n);
+    return cudaGetLastError();
+}
+
+}  // namespace parw2v

@@ -172,3 +172,74 @@ def write_text(path: str, tokens: np.ndarray, lengths: np.ndarray, prefix: str =
             f.write(s)
             total += len(s)
     return total
+
+
+def topic_zipf_stream_torch(n_tokens: int, n_types: int, n_topics: int, *, lognormal_mean: float = 25.0,
+                            lognormal_sigma: float = 1.0, p_global: float = 0.5, s: float = 1.0, seed: int = 4,
+                            min_count: int = 5, device: str = "cuda"):
+    """The 1B-word-shaped corpus built directly as a vocabulary-id stream on the GPU.
+
+    Same generator as ``topic_zipf`` with lognormal sentence lengths; the vocabulary step is
+    the reference's (counts, "</s>" first, descending count, min_count filter), with ties in
+    count ordered by generator id (the text path orders ties as the reference's qsort does).
+    Returns ``(stream_int32_device, counts_uint32_numpy, words_list, gen_ids_of_rows)`` where
+    the stream holds one 0 ("</s>") after every sentence.
+    """
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    mu = float(np.log(lognormal_mean) - 0.5 * lognormal_sigma ** 2)
+    est = int(n_tokens / lognormal_mean * 1.1) + 1024
+    lengths = torch.empty(0, dtype=torch.int64, device=device)
+    while int(lengths.sum()) < n_tokens:
+        more = torch.empty(est, device=device, dtype=torch.float64).log_normal_(mu, lognormal_sigma, generator=g)
+        lengths = torch.cat([lengths, more.round().clamp_(1, 1000).to(torch.int64)])
+    csum = torch.cumsum(lengths, 0)
+    k = int(torch.searchsorted(csum, torch.tensor([n_tokens], device=device)).item())
+    lengths = lengths[: k + 1].clone()
+    lengths[-1] -= int(csum[k].item()) - n_tokens
+    lengths = lengths[lengths > 0]
+    n_sent = len(lengths)
+    topic = torch.randint(0, n_topics, (n_sent,), generator=g, device=device)
+    g_cdf = torch.from_numpy(_zipf_cdf(n_types, s)).to(device)
+    slice_len = -(-n_types // n_topics)
+    l_cdf = torch.from_numpy(_zipf_cdf(slice_len, s)).to(device)
+    ids = torch.empty(n_tokens, dtype=torch.int64, device=device)
+    chunk = 1 << 27
+    tok_topic_all = torch.repeat_interleave(topic, lengths)
+    for s0 in range(0, n_tokens, chunk):
+        s1 = min(n_tokens, s0 + chunk)
+        m = s1 - s0
+        u = torch.rand(m, generator=g, device=device, dtype=torch.float64)
+        use_g = torch.rand(m, generator=g, device=device) < p_global
+        gi = torch.searchsorted(g_cdf, u, right=True).clamp_(max=n_types - 1)
+        li = torch.searchsorted(l_cdf, u, right=True).clamp_(max=slice_len - 1)
+        tt = tok_topic_all[s0:s1]
+        loc = tt + n_topics * li
+        loc = torch.where(loc >= n_types, tt, loc)
+        ids[s0:s1] = torch.where(use_g, gi, loc)
+    del tok_topic_all
+    cnt = torch.bincount(ids, minlength=n_types)
+    # vocabulary order: descending count, ties by generator id; "</s>" is row 0
+    order = torch.argsort(-cnt * (n_types + 1) + torch.arange(n_types, device=device))
+    cnt_sorted = cnt[order]
+    keep = cnt_sorted >= min_count
+    order = order[keep]
+    row_of = torch.full((n_types,), -1, dtype=torch.int64, device=device)
+    row_of[order] = torch.arange(1, len(order) + 1, device=device)
+    rows = row_of[ids]
+    del ids
+    # stream: sentence tokens followed by a 0, dropping filtered (-1) words
+    ends = torch.cumsum(lengths + 1, 0) - 1
+    stream = torch.empty(n_tokens + n_sent, dtype=torch.int64, device=device)
+    is_end = torch.zeros(n_tokens + n_sent, dtype=torch.bool, device=device)
+    is_end[ends] = True
+    stream[is_end] = 0
+    stream[~is_end] = rows
+    del rows
+    stream = stream[stream >= 0].to(torch.int32)
+    counts = np.concatenate([[n_sent], cnt[order].cpu().numpy()]).astype(np.uint32)
+    gen_ids = order.cpu().numpy()
+    words = [b"</s>"] + [b"w%d" % i for i in gen_ids.tolist()]
+    return stream, counts, words, gen_ids
