@@ -60,6 +60,9 @@ typedef struct {
     int grid;        /* Hogwild modes: persistent CTAs, 0 = one wave of the device */
     int warps_per_cta; /* Hogwild modes: sentences in flight per CTA, 0 = tuned default */
     size_t mem_cap_bytes; /* refuse device allocations beyond this total, 0 = no cap */
+    int min_rounds;  /* Hogwild modes: sentences in flight are capped at lines / min_rounds so that
+                        a small corpus is not processed almost all at once from stale weights
+                        (0 = 256, negative = no cap) */
 } parw2v_config;
 
 typedef struct {

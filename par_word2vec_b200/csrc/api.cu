@@ -33,7 +33,7 @@ struct parw2v_ctx {
     bool weights_ready = false;
     // corpus and packing
     int32_t *d_corpus = nullptr;
-    uint64_t n_tokens = 0, corpus_cap = 0;
+    uint64_t n_tokens = 0, corpus_cap = 0, n_lines = 0;
     int32_t *d_packed = nullptr;
     uint32_t *d_line_end = nullptr;
     uint64_t line_cap = 0;
@@ -48,6 +48,7 @@ struct parw2v_ctx {
     DevTrace dtr;
     size_t trace_bytes = 0;
     void *d_trace_mem = nullptr;
+    int last_grid = 0, last_warps = 0;  // launch shape of the last Hogwild training call
 };
 
 static std::string g_create_error;
@@ -378,13 +379,18 @@ int parw2v_set_trace(parw2v_ctx *c, parw2v_trace *t) {
 }
 
 // Validation of token ids against the vocabulary (one pass, on the device).
+// Validation of token ids against the vocabulary and count of "</s>"-terminated lines (one pass).
 __global__ void k_validate(const int32_t *corpus, uint64_t n, int V, DevCounters *cnt) {
     bool bad = false;
+    unsigned long long lines = 0;
     for (uint64_t i = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t) gridDim.x * blockDim.x) {
         const int w = corpus[i];
         bad |= (w < 0 || w >= V);
+        lines += (w == 0);
     }
+    for (int o = 16; o > 0; o >>= 1) lines += __shfl_xor_sync(0xffffffffu, lines, o);
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&cnt->error, kErrCapacity);
+    if ((threadIdx.x & 31) == 0 && lines) atomicAdd(&cnt->n_lines, lines);
 }
 
 static int read_counters(parw2v_ctx *c, DevCounters *h) {
@@ -517,7 +523,7 @@ static int train_hogwild(parw2v_ctx *c, TrainArgs &a, parw2v_stats *st) {
     int warps = c->cfg.warps_per_cta;
     const bool plain = c->cfg.mode == PARW2V_MODE_PLAIN;
     if (plain) {
-        warps = plain_warps_per_cta();
+        warps = plain_warps_per_cta(warps);
         if (!grid) grid = sms * 2;
         const size_t per = plain_scratch_floats(c->ld, c->cfg.batch_size, c->cfg.window, c->cfg.negative);
         const size_t need = per * (size_t) grid * warps;
@@ -537,6 +543,22 @@ static int train_hogwild(parw2v_ctx *c, TrainArgs &a, parw2v_stats *st) {
         if (!warps || warps > maxw) warps = maxw;
         if (!grid) grid = sms;
     }
+    // cap the sentences in flight at lines / min_rounds (see parw2v_config.min_rounds)
+    const int min_rounds = c->cfg.min_rounds == 0 ? 256 : c->cfg.min_rounds;
+    if (min_rounds > 0) {
+        const uint64_t cap = std::max<uint64_t>(1, c->n_lines / (uint64_t) min_rounds);
+        if ((uint64_t) grid * warps > cap) {
+            if (cap < (uint64_t) sms) {
+                warps = 1;
+                grid = (int) cap;
+            } else {
+                warps = std::max(1, std::min(warps, (int) (cap / (uint64_t) sms)));
+                grid = (int) std::max<uint64_t>(1, cap / (uint64_t) warps);
+            }
+        }
+    }
+    c->last_grid = grid;
+    c->last_warps = warps;
     float pack_ms_total = 0.f, kernel_ms_total = 0.f;
     for (int ep = 0; ep < c->cfg.iter; ep++) {
         a.epoch = ep;
@@ -590,6 +612,7 @@ int parw2v_train(parw2v_ctx *c, parw2v_stats *st) {
     DevCounters h;
     if ((rc = read_counters(c, &h))) return rc;
     if (h.error & kErrCapacity) return fail(c, PARW2V_ERR_ARG, "corpus holds ids outside [0, vocab_size)");
+    c->n_lines = h.n_lines;
     TrainArgs a{};
     a.corpus = c->d_corpus;
     a.n_tokens = c->n_tokens;

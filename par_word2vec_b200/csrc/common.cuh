@@ -73,3 +73,52 @@ __device__ __forceinline__ void red_add_f2(float *addr, float2 v) {
 }
 
 }  // namespace parw2v
+
+namespace parw2v {
+
+// The shared negatives of one repulsion batch (PAR_Word2Vec_cpu.cpp:603-622), drawn by a warp with
+// the reference's exact random stream.  Draw k uses LCG state rng_{k+1}; every lane jumps to its
+// own state and reads the unigram table at once (one memory latency instead of K dependent ones).
+// The candidates are checked against the sentence; the first one found in it is resolved the
+// reference's way (uniform redraws until a word outside the sentence), which shifts the stream,
+// so the draws after it are redone from the new state.  Returns false if a redraw loop exceeds
+// max_resample draws (the reference would spin forever when every word is in the sentence).
+__device__ __forceinline__ bool warp_draw_negatives(const int32_t *table, int vocab, uint64_t &rng, const int *sen,
+                                                    int len, int K, int *negs, int lane, int64_t max_resample) {
+    int k0 = 0;
+    while (k0 < K) {
+        const int nk = min(K - k0, 32);
+        int cand = -1;
+        if (lane < nk) {
+            const uint64_t r = lcg_jump(rng, (uint64_t) lane + 1);
+            cand = __ldg(table + (r >> 16) % (uint64_t) kTableSize);
+            if (!cand) cand = (int) (r % (uint64_t) (vocab - 1) + 1);
+        }
+        bool hit = false;
+        for (int q = 0; q < len; q++) hit |= (sen[q] == cand);
+        const unsigned m = __ballot_sync(0xffffffffu, hit && lane < nk);
+        const int first = m ? __ffs(m) - 1 : nk;
+        if (lane < first) negs[k0 + lane] = cand;
+        if (first == nk) {
+            rng = lcg_jump(rng, (uint64_t) nk);
+            k0 += nk;
+            continue;
+        }
+        rng = lcg_jump(rng, (uint64_t) first + 1);
+        int s = 0;
+        for (int64_t tries = 0;; tries++) {
+            if (tries >= max_resample) return false;
+            rng = lcg_next(rng);
+            s = (int) (rng % (uint64_t) (vocab - 1) + 1);
+            bool h2 = false;
+            for (int q = lane; q < len; q += 32) h2 |= (sen[q] == s);
+            if (!__any_sync(0xffffffffu, h2)) break;
+        }
+        if (lane == 0) negs[k0 + first] = s;
+        k0 += first + 1;
+    }
+    __syncwarp();
+    return true;
+}
+
+}  // namespace parw2v

@@ -71,7 +71,7 @@ uint64_t pack_tiles(uint64_t n_tokens);
 cudaError_t launch_plain_train(const TrainArgs &a, int grid, int warps_per_cta, cudaStream_t s);
 cudaError_t launch_batched_train(const TrainArgs &a, bool bf16, int grid, int warps_per_cta, cudaStream_t s);
 size_t plain_scratch_floats(int ld, int batch, int window, int negative);
-int plain_warps_per_cta();
+int plain_warps_per_cta(int requested);
 int batched_max_warps(int ld, int window, int negative, int batch, bool bf16, size_t *smem_per_warp);
 
 // Loss / adjoint / finite differences

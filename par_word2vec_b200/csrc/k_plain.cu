@@ -9,7 +9,10 @@
 //   repulsion   per batch of `batch` positions: rep_b and rep_b * negative shared negatives from
 //               the unigram table, redrawn uniformly while they occur in the sentence; M_in and
 //               M_out are staged in the warp's global workspace, the three products run on the
-//               warp, and the updates are added with vector red.global.add.
+//               warp.  Each touched row is written back once as (staged value + this batch's
+//               update), duplicates merged first: concurrent writers of a hot row then lose
+//               updates, as the reference's unsynchronised `+=` does, instead of summing
+//               thousands of updates computed from the same stale value (which diverges).
 // Random streams: the sentence's LCG starts from mix64(seed, epoch, line, piece); the learning
 // rate decays linearly with the sentence's position in the corpus (the reference decays with the
 // words processed so far, :443).
@@ -66,45 +69,67 @@ __device__ __forceinline__ uint64_t sentence_seed(const TrainArgs &a, uint64_t l
     return mix64(mix64(a.seed ^ (0xD1B54A32D192ED03ULL * (uint64_t) (a.epoch + 1))) ^ (line * 1024ULL + piece));
 }
 
-// Shared negative draw (PAR_Word2Vec_cpu.cpp:603-622) with the membership test spread over the warp.
-__device__ __forceinline__ int draw_negative(const TrainArgs &a, uint64_t &rng, const int *sen, int len, int lane,
-                                             bool &failed) {
-    rng = lcg_next(rng);
-    int s = __ldg(a.table + (rng >> 16) % (uint64_t) kTableSize);
-    if (!s) s = (int) (rng % (uint64_t) (a.vocab - 1) + 1);
-    for (int64_t tries = 0;; tries++) {
-        bool hit = false;
-        for (int q = lane; q < len; q += 32) hit |= (sen[q] == s);
-        if (!__any_sync(0xffffffffu, hit)) break;
-        if (tries >= a.max_resample) {
-            failed = true;
-            break;
-        }
-        rng = lcg_next(rng);
-        s = (int) (rng % (uint64_t) (a.vocab - 1) + 1);
+__host__ __device__ __forceinline__ size_t plain_warp_smem(int kmax, int B) {
+    return sizeof(int) * (size_t) (kMaxSentence + 2 * kmax + B) + sizeof(float) * (size_t) kmax * B;
+}
+
+// Duplicate words among the batch's negatives (and among its rows) would write the same row twice;
+// their gradient rows / columns are merged into the first occurrence, which then writes once.
+__device__ __forceinline__ void merge_duplicates(const int *negs, int K, const int *sen_b, int rows, float *grad,
+                                                 int *dup, int lane) {
+    for (int k = lane; k < K; k += 32) {
+        int first = -1;
+        for (int q = 0; q < k && first < 0; q++)
+            if (negs[q] == negs[k]) first = q;
+        dup[k] = first;
     }
-    return s;
+    for (int r = lane; r < rows; r += 32) {
+        int first = -1;
+        for (int q = 0; q < r && first < 0; q++)
+            if (sen_b[q] == sen_b[r]) first = q;
+        dup[K + r] = first;
+    }
+    __syncwarp();
+    // columns (batch rows) first, then rows (negatives): each step keeps G consistent
+    for (int r = 0; r < rows; r++) {
+        const int f = dup[K + r];
+        if (f >= 0)
+            for (int k = lane; k < K; k += 32) {
+                grad[k * rows + f] += grad[k * rows + r];
+                grad[k * rows + r] = 0.f;
+            }
+        __syncwarp();
+    }
+    for (int k = 0; k < K; k++) {
+        const int f = dup[k];
+        if (f >= 0)
+            for (int r = lane; r < rows; r += 32) {
+                grad[f * rows + r] += grad[k * rows + r];
+                grad[k * rows + r] = 0.f;
+            }
+        __syncwarp();
+    }
 }
 
 template <int NV2>
-__global__ void __launch_bounds__(kPlainWarps * 32) k_plain_train(TrainArgs a) {
+__global__ void __launch_bounds__(kPlainWarps * 32) k_plain_train(TrainArgs a, int warps) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int w = a.window, B = a.batch, ld = a.ld;
     const int n2 = (a.d + 1) >> 1;
     const int kmax = 2 * w * a.negative;
     float *s_exp = reinterpret_cast<float *>(smem_raw);  // 1004
-    unsigned char *warp_base = smem_raw + 1004 * sizeof(float) +
-                               (size_t) wid * (sizeof(int) * (kMaxSentence + kmax) + sizeof(float) * kmax * B);
+    unsigned char *warp_base = smem_raw + 1004 * sizeof(float) + (size_t) wid * plain_warp_smem(kmax, B);
     int *sen = reinterpret_cast<int *>(warp_base);
     int *negs = sen + kMaxSentence;
-    float *grad = reinterpret_cast<float *>(negs + kmax);
+    int *dup = negs + kmax;  // kmax + B: duplicate marks of negatives, then of batch rows
+    float *grad = reinterpret_cast<float *>(dup + kmax + B);
     for (int i = threadIdx.x; i <= kExpTableSize; i += blockDim.x) s_exp[i] = a.exp_table[i];
     __syncthreads();
 
     float *w_in = static_cast<float *>(a.w_in);
     float *w_out = static_cast<float *>(a.w_out);
-    const size_t gwarp = (size_t) blockIdx.x * kPlainWarps + wid;
+    const size_t gwarp = (size_t) blockIdx.x * warps + wid;
     float *m_in = a.scratch + gwarp * a.scratch_per_warp;  // B x ld
     float *m_out = m_in + (size_t) B * ld;                  // kmax x ld
     const uint64_t n_lines = a.cnt->n_lines, total_kept = a.cnt->total_kept;
@@ -162,9 +187,9 @@ __global__ void __launch_bounds__(kPlainWarps * 32) k_plain_train(TrainArgs a) {
                 const int rep_b = (lo_b <= w - 1 || (L - 1) - lo_b <= w - 1) ? (int) (rng % (uint64_t) w)
                                                                               : (int) (rng % (uint64_t) (2 * w));
                 const int K = rep_b * a.negative;
-                for (int k = 0; k < K; k++) {
-                    const int s = draw_negative(a, rng, sen, L, lane, failed);
-                    if (lane == 0) negs[k] = s;
+                if (!warp_draw_negatives(a.table, a.vocab, rng, sen, L, K, negs, lane, a.max_resample)) {
+                    failed = true;  // unresolved negatives: leave the batch untouched
+                    break;
                 }
                 st_batches++;
                 st_negs += K;
@@ -193,11 +218,12 @@ __global__ void __launch_bounds__(kPlainWarps * 32) k_plain_train(TrainArgs a) {
                     }
                 }
                 __syncwarp();
-                // MM2: W_out[neg_k] += sum_r grad[k][r] M_in[r]
+                merge_duplicates(negs, K, sen + lo_b, rows, grad, dup, lane);
+                // MM2: W_out[neg_k] = M_out[k] + sum_r grad[k][r] M_in[r]  (each distinct word once)
                 for (int k = 0; k < K; k++) {
+                    if (dup[k] >= 0) continue;
                     RowReg<NV2> acc;
-#pragma unroll
-                    for (int q = 0; q < NV2; q++) acc.v[q] = make_float2(0.f, 0.f);
+                    load_row(acc, m_out + (size_t) k * ld, n2, lane);
                     for (int r = 0; r < rows; r++) {
                         RowReg<NV2> in;
                         load_row(in, m_in + (size_t) r * ld, n2, lane);
@@ -206,16 +232,13 @@ __global__ void __launch_bounds__(kPlainWarps * 32) k_plain_train(TrainArgs a) {
                         for (int q = 0; q < NV2; q++)
                             acc.v[q] = make_float2(fmaf(g, in.v[q].x, acc.v[q].x), fmaf(g, in.v[q].y, acc.v[q].y));
                     }
-                    float *dst = w_out + (size_t) negs[k] * ld;
-#pragma unroll
-                    for (int q = 0; q < NV2; q++)
-                        if (lane + 32 * q < n2) red_add_f2(dst + 2 * (lane + 32 * q), acc.v[q]);
+                    store_row(acc, w_out + (size_t) negs[k] * ld, n2, lane);
                 }
-                // MM3: W_in[sen[lo_b + r]] += sum_k grad[k][r] M_out[k]
+                // MM3: W_in[sen[lo_b + r]] = M_in[r] + sum_k grad[k][r] M_out[k]
                 for (int r = 0; r < rows; r++) {
+                    if (dup[K + r] >= 0) continue;
                     RowReg<NV2> acc;
-#pragma unroll
-                    for (int q = 0; q < NV2; q++) acc.v[q] = make_float2(0.f, 0.f);
+                    load_row(acc, m_in + (size_t) r * ld, n2, lane);
                     for (int k = 0; k < K; k++) {
                         RowReg<NV2> o;
                         load_row(o, m_out + (size_t) k * ld, n2, lane);
@@ -224,10 +247,7 @@ __global__ void __launch_bounds__(kPlainWarps * 32) k_plain_train(TrainArgs a) {
                         for (int q = 0; q < NV2; q++)
                             acc.v[q] = make_float2(fmaf(g, o.v[q].x, acc.v[q].x), fmaf(g, o.v[q].y, acc.v[q].y));
                     }
-                    float *dst = w_in + (size_t) sen[lo_b + r] * ld;
-#pragma unroll
-                    for (int q = 0; q < NV2; q++)
-                        if (lane + 32 * q < n2) red_add_f2(dst + 2 * (lane + 32 * q), acc.v[q]);
+                    store_row(acc, w_in + (size_t) sen[lo_b + r] * ld, n2, lane);
                 }
                 __syncwarp();
             }
@@ -248,13 +268,11 @@ __global__ void __launch_bounds__(kPlainWarps * 32) k_plain_train(TrainArgs a) {
 
 template <int NV2>
 cudaError_t launch_plain_nv(const TrainArgs &a, int grid, int warps, cudaStream_t s) {
-    (void) warps;
     const int kmax = 2 * a.window * a.negative;
-    const size_t smem = 1004 * sizeof(float) +
-                        (size_t) kPlainWarps * (sizeof(int) * (kMaxSentence + kmax) + sizeof(float) * kmax * a.batch);
+    const size_t smem = 1004 * sizeof(float) + (size_t) warps * plain_warp_smem(kmax, a.batch);
     cudaError_t e = cudaFuncSetAttribute(k_plain_train<NV2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
     if (e != cudaSuccess) return e;
-    k_plain_train<NV2><<<grid, kPlainWarps * 32, smem, s>>>(a);
+    k_plain_train<NV2><<<grid, warps * 32, smem, s>>>(a, warps);
     return cudaGetLastError();
 }
 
@@ -264,7 +282,7 @@ size_t plain_scratch_floats(int ld, int batch, int window, int negative) {
     return (size_t) (batch + 2 * window * negative) * ld;
 }
 
-int plain_warps_per_cta() { return kPlainWarps; }
+int plain_warps_per_cta(int requested) { return requested > 0 && requested < kPlainWarps ? requested : kPlainWarps; }
 
 cudaError_t launch_plain_train(const TrainArgs &a, int grid, int warps_per_cta, cudaStream_t s) {
     const int nv2 = (a.d + 63) / 64;
