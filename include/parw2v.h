@@ -63,7 +63,16 @@ typedef struct {
     int min_rounds;  /* Hogwild modes: sentences in flight are capped at lines / min_rounds so that
                         a small corpus is not processed almost all at once from stale weights
                         (0 = 256, negative = no cap) */
+    int attraction;  /* PARW2V_ATTRACT_*: how the contexts of one target are applied */
 } parw2v_config;
+
+/* Attraction variants (cfg.attraction) */
+#define PARW2V_ATTRACT_DEFAULT 0    /* SEQUENTIAL in DET/PLAIN, WINDOW in the BATCHED modes */
+#define PARW2V_ATTRACT_SEQUENTIAL 1 /* the reference: each context sees the target row as the
+                                       previous context left it (cpu.cpp:536-567) */
+#define PARW2V_ATTRACT_WINDOW 2     /* window-synchronous: all contexts of a target are scored
+                                       against the same target row, then all updates are applied
+                                       (the contexts x d by d x 1 contraction of the window) */
 
 typedef struct {
     uint64_t words;      /* raw tokens read incl. "</s>" over all epochs: the reference's

@@ -128,6 +128,57 @@ static uint64_t read_sentence(trainer *t, const int32_t *stream, uint64_t word_c
     return word_count;
 }
 
+/* Window-synchronous attraction (the BATCHED modes' option): every context c of the target is
+ * scored against the target row y as it was before this position, f_c = x_c . y (sequential sum),
+ * g_c from the table; then y += sum_c g_c x_c (contexts in window order, x_c before update) and
+ * x_c += g_c y for each distinct context word (a word occurring twice gets the sum of its g). */
+static void attract_sync(trainer *t, int pos, int b, int target) {
+    const int d = t->cfg->hidden_size, w = t->cfg->window;
+    int ctx[256];
+    float g[256];
+    int n = 0;
+    float *y = t->w_out + (int64_t) target * d;
+    for (int i = b; i < 2 * w + 1 - b && n < 256; i++) {
+        if (i == w) continue;
+        const int c = pos - w + i;
+        if (c < 0) continue;
+        if (c >= t->len) break;
+        const float *x = t->w_in + (int64_t) t->sen[c] * d;
+        float f = 0.f;
+        for (int j = 0; j < d; j++) {
+            float p = x[j] * y[j];
+            f = f + p;
+        }
+        ctx[n] = t->sen[c];
+        g[n] = grad_of(f, 1, t->alpha, t->exp_table);
+        n++;
+        if (t->tr) t->tr->n_pairs++;
+    }
+    for (int i = 0; i < n; i++)  /* merge repeated context words into their first occurrence */
+        for (int k = 0; k < i; k++)
+            if (ctx[k] == ctx[i]) {
+                g[k] = g[k] + g[i];
+                g[i] = 0.f;
+                break;
+            }
+    for (int j = 0; j < d; j++) {
+        const float yj = y[j];
+        float dy = 0.f;
+        for (int i = 0; i < n; i++) {
+            float *x = t->w_in + (int64_t) ctx[i] * d;
+            float p = g[i] * x[j];
+            dy = dy + p;
+        }
+        for (int i = 0; i < n; i++) {
+            if (g[i] == 0.f) continue;
+            float *x = t->w_in + (int64_t) ctx[i] * d;
+            float p = g[i] * yj;
+            x[j] = x[j] + p;
+        }
+        y[j] = yj + dy;
+    }
+}
+
 /* One attraction step for sentence position pos, PAR_Word2Vec_cpu.cpp:529-568 */
 static void attract(trainer *t, int pos) {
     const int d = t->cfg->hidden_size, w = t->cfg->window;
@@ -138,6 +189,10 @@ static void attract(trainer *t, int pos) {
         trace_u8(t->tr->b, t->tr->b_cap, &t->tr->n_b, (uint8_t) b);
         if (t->tr->alpha && t->tr->n_alpha < t->tr->alpha_cap) t->tr->alpha[t->tr->n_alpha] = t->alpha;
         t->tr->n_alpha++;
+    }
+    if (t->cfg->sync_window) {
+        attract_sync(t, pos, b, target);
+        return;
     }
     for (int i = b; i < 2 * w + 1 - b; i++) {
         if (i == w) continue;

@@ -32,6 +32,10 @@ typedef struct {
     float alpha;         /* -alpha */
     float sample;        /* -sample */
     uint64_t seed;       /* initial LCG state; the reference uses the OpenMP thread id (0) */
+    int sync_window;     /* 0: the reference's attraction (each context sees the target row as the
+                            previous context left it); 1: window-synchronous variant (all contexts
+                            of a target are scored against the same target row, then every update
+                            is applied; repeated context words accumulate into one row) */
 } pwo_config;
 
 /* Optional trace.  Each array may be NULL; entries beyond *_cap are counted, not stored. */

@@ -21,7 +21,8 @@ TABLE_SIZE = 100_000_000
 class Config(ctypes.Structure):
     _fields_ = [("vocab_size", ctypes.c_int), ("hidden_size", ctypes.c_int), ("window", ctypes.c_int),
                 ("negative", ctypes.c_int), ("batch_size", ctypes.c_int), ("iter", ctypes.c_int),
-                ("alpha", ctypes.c_float), ("sample", ctypes.c_float), ("seed", ctypes.c_uint64)]
+                ("alpha", ctypes.c_float), ("sample", ctypes.c_float), ("seed", ctypes.c_uint64),
+                ("sync_window", ctypes.c_int)]
 
 
 class Trace(ctypes.Structure):
@@ -82,14 +83,14 @@ def init_net(vocab_size: int, size: int):
 
 
 def train(counts, stream_with_sentinel, w_in, w_out, *, size, window, negative, batch_size, iter, alpha, sample,
-          seed=0, table=None, trace_caps=None, max_resample=0):
+          seed=0, table=None, trace_caps=None, max_resample=0, sync_window=0):
     """Run the restated loop in place on w_in / w_out; returns the trace dict."""
     c = np.ascontiguousarray(counts, np.uint32)
     s = np.ascontiguousarray(stream_with_sentinel, np.int32)
     if table is None:
         table = unigram_table(c)
     et = exp_table()
-    cfg = Config(len(c), size, window, negative, batch_size, iter, alpha, sample, seed)
+    cfg = Config(len(c), size, window, negative, batch_size, iter, alpha, sample, seed, int(sync_window))
     caps = trace_caps or {}
     bufs = dict(keep=np.zeros(caps.get("keep", 0), np.uint8), b=np.zeros(caps.get("b", 0), np.uint8),
                 alpha=np.zeros(caps.get("alpha", 0), np.float32), rep_b=np.zeros(caps.get("rep_b", 0), np.uint8),

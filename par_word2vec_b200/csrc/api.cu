@@ -135,6 +135,8 @@ int parw2v_create(const parw2v_config *cfg, parw2v_ctx **out) {
         k.sample < 0 || k.mode < PARW2V_MODE_DET || k.mode > PARW2V_MODE_BATCHED_BF16 || k.grid < 0 ||
         k.warps_per_cta < 0)
         return fail(nullptr, PARW2V_ERR_ARG, "invalid configuration value");
+    if (k.attraction < PARW2V_ATTRACT_DEFAULT || k.attraction > PARW2V_ATTRACT_WINDOW)
+        return fail(nullptr, PARW2V_ERR_ARG, "invalid attraction variant");
     if (k.window > 100 || k.negative > 100 || k.batch_size > 1000)
         return fail(nullptr, PARW2V_ERR_CAPACITY, "window/negative/batch_size beyond the supported range");
     if (k.mode != PARW2V_MODE_DET && k.size > 512)
@@ -636,6 +638,11 @@ int parw2v_train(parw2v_ctx *c, parw2v_stats *st) {
     a.packed = c->d_packed;
     a.line_end = c->d_line_end;
     a.max_resample = 1LL << 20;
+    {
+        const bool batched = c->cfg.mode == PARW2V_MODE_BATCHED || c->cfg.mode == PARW2V_MODE_BATCHED_BF16;
+        a.sync_window = c->cfg.attraction == PARW2V_ATTRACT_WINDOW ||
+                        (c->cfg.attraction == PARW2V_ATTRACT_DEFAULT && batched);
+    }
     if (c->cfg.mode == PARW2V_MODE_DET) return train_det(c, a, st);
     rc = ensure_packing(c);
     if (rc) return rc;

@@ -40,6 +40,14 @@ __host__ __device__ inline uint64_t lcg_jump(uint64_t x, uint64_t n) {
     return acc.a * x + acc.c;
 }
 
+// x mod m for a 64-bit x and 0 < m < 2^16, exactly, through 32-bit remainders:
+// (hi * 2^32 + lo) mod m = ((hi mod m) * (2^32 mod m) + lo mod m) mod m, all terms < 2^32.
+__host__ __device__ __forceinline__ uint32_t mod_small(uint64_t x, uint32_t m) {
+    const uint32_t r32 = (uint32_t) (0x100000000ULL % m);
+    const uint32_t hi = (uint32_t) (x >> 32) % m, lo = (uint32_t) x % m;
+    return (hi * r32 % m + lo) % m;
+}
+
 // SplitMix64 finaliser (Steele, Lea & Flood 2014): a bijective 64-bit mixer used to derive
 // independent per-token / per-sentence random streams in the Hogwild modes.
 __host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
@@ -83,7 +91,7 @@ namespace parw2v {
 // reference's way (uniform redraws until a word outside the sentence), which shifts the stream,
 // so the draws after it are redone from the new state.  Returns false if a redraw loop exceeds
 // max_resample draws (the reference would spin forever when every word is in the sentence).
-__device__ __forceinline__ bool warp_draw_negatives(const int32_t *table, int vocab, uint64_t &rng, const int *sen,
+static __device__ __noinline__ bool warp_draw_negatives(const int32_t *table, int vocab, uint64_t &rng, const int *sen,
                                                     int len, int K, int *negs, int lane, int64_t max_resample) {
     int k0 = 0;
     while (k0 < K) {

@@ -54,6 +54,7 @@ struct TrainArgs {
     float *scratch;          // per-warp workspace (PLAIN), per-context workspace (DET)
     size_t scratch_per_warp; // floats
     int64_t max_resample;
+    int sync_window;         // window-synchronous attraction (PARW2V_ATTRACT_WINDOW)
 };
 
 // Launchers (return a cudaError_t)

@@ -35,13 +35,26 @@ constexpr int kRing = kPrefetch + 1;          // landing buffers for targets / B
 constexpr int kMaxWarpsB = 16;
 constexpr size_t kSmemBudget = 227 * 1024;
 
+// Tensor-core repulsion (BF16 mode): shapes and staging geometry
+constexpr int kMmaK = 48;        // negatives per batch handled by the mma path (3 m-tiles)
+constexpr int kMmaR = 32;        // batch rows handled by the mma path (2 m-tiles / 4 n-tiles)
+constexpr int kMmaCols = 64;     // column chunk of the staging
+constexpr int kMmaStride = 72;   // staged row stride in bf16 (144 B: conflict-free ldmatrix rows)
+constexpr int kGbStride = 40;    // bf16 G row stride (80 B)
+
+__host__ __device__ inline bool mma_path(int kmax_eff, int batch, bool bf16) {
+    return bf16 && kmax_eff <= kMmaK && batch <= kMmaR;
+}
+
 struct Layout {  // per-warp shared-memory carve-up, in bytes (all offsets 16-byte aligned)
     int ws;            // window slots 2w+1+P
-    int ch;            // repulsion column chunk (multiple of 4)
+    int ch;            // repulsion column chunk (multiple of 4), SIMT path
     int kmax;          // 2 * window * negative
-    size_t region;     // window cur rows (+ BF16 landing ring) | repulsion chunk staging
+    bool mma;          // tensor-core repulsion
+    size_t region;     // window cur rows (+ BF16 landing ring) | repulsion staging
     size_t raw_off;    // BF16 landing ring inside the region
-    size_t tgt_off, g_off, neg_off, dup_off, meta_off, exit_off, per_warp;
+    size_t gb_off;     // mma path: bf16 G inside the region, after the staged chunk
+    size_t tgt_off, g_off, neg_off, dup_off, meta_off, ctx_off, exit_off, per_warp;
 };
 
 __host__ __device__ inline size_t up16(size_t x) { return (x + 15) & ~(size_t) 15; }
@@ -61,14 +74,23 @@ __host__ __device__ inline Layout make_layout(int ld, int window, int negative, 
     if (ch > ((ld + 3) / 4) * 4) ch = ((ld + 3) / 4) * 4;
     if (ch < 16) ch = 16;
     L.ch = (int) ch;
-    const size_t rep_bytes = up16(rows_rep * (size_t) (L.ch + 4) * 4);
+    L.mma = mma_path((2 * window - 1) * negative, batch, bf16);
+    size_t rep_bytes = up16(rows_rep * (size_t) (L.ch + 4) * 4);
+    L.gb_off = 0;
+    if (L.mma) {
+        const size_t stage = up16((size_t) (kMmaR + kMmaK) * kMmaStride * 2);
+        L.gb_off = stage;
+        rep_bytes = stage + up16((size_t) kMmaK * kGbStride * 2);
+    }
     L.region = win_total > rep_bytes ? win_total : rep_bytes;
     L.tgt_off = L.region;
     L.g_off = L.tgt_off + up16((size_t) kRing * row_st);
-    L.neg_off = L.g_off + up16((size_t) L.kmax * batch * 4);
+    const size_t g_floats = L.mma ? (size_t) kMmaK * kMmaR : (size_t) L.kmax * batch;
+    L.neg_off = L.g_off + up16(g_floats * 4);
     L.dup_off = L.neg_off + up16((size_t) L.kmax * 4);
     L.meta_off = L.dup_off + up16((size_t) (L.kmax + batch) * 4);
-    L.exit_off = L.meta_off + up16((size_t) L.ws * 8);
+    L.ctx_off = L.meta_off + up16((size_t) L.ws * 8);
+    L.exit_off = L.ctx_off + up16((size_t) (2 * window) * 8);
     L.per_warp = L.exit_off + up16((size_t) kPrefetch * 4 + 16);
     return L;
 }
@@ -147,7 +169,327 @@ __device__ __forceinline__ uint64_t sentence_seed_b(const TrainArgs &a, uint64_t
     return mix64(mix64(a.seed ^ (0xD1B54A32D192ED03ULL * (uint64_t) (a.epoch + 1))) ^ (line * 1024ULL + piece));
 }
 
-template <int NV2, bool BF16>
+// Per-lane stream of random bits for stochastic rounding (xorshift64*, Vigna 2016).
+struct LaneBits {
+    uint64_t s;
+    __device__ __forceinline__ uint64_t next() {
+        s ^= s >> 12;
+        s ^= s << 25;
+        s ^= s >> 27;
+        return s * 0x2545F4914F6CDD1DULL;
+    }
+};
+
+__device__ __forceinline__ void ldsm_x4(unsigned (&r)[4], const void *p) {
+    const unsigned a = (unsigned) __cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(a));
+}
+__device__ __forceinline__ void ldsm_x4_t(unsigned (&r)[4], const void *p) {
+    const unsigned a = (unsigned) __cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(a));
+}
+__device__ __forceinline__ void ldsm_x2_t(unsigned (&r)[2], const void *p) {
+    const unsigned a = (unsigned) __cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0,%1}, [%2];" : "=r"(r[0]), "=r"(r[1]) : "r"(a));
+}
+// D += A (16x16 bf16, row) * B (16x8 bf16, col), FP32 accumulate
+__device__ __forceinline__ void mma16816(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                 "{%0,%1,%2,%3};"
+                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Merge gradient rows of repeated negatives and gradient columns of repeated batch words into
+// their first occurrence (G is K x rows with row stride gs), so each distinct row is written once.
+__device__ __noinline__ void merge_repeats(const int *negs, int K, const int32_t *batch_words, int rows, float *G,
+                                              int gs, int *dup, int lane) {
+    for (int k = lane; k < K; k += 32) {
+        int first = -1;
+        for (int q = 0; q < k && first < 0; q++)
+            if (negs[q] == negs[k]) first = q;
+        dup[k] = first;
+    }
+    for (int r = lane; r < rows; r += 32) {
+        int first = -1;
+        const int wr = __ldg(batch_words + r);
+        for (int q = 0; q < r && first < 0; q++)
+            if (__ldg(batch_words + q) == wr) first = q;
+        dup[K + r] = first;
+    }
+    __syncwarp();
+    for (int r = 0; r < rows; r++) {
+        const int f = dup[K + r];
+        if (f >= 0)
+            for (int k = lane; k < K; k += 32) {
+                G[k * gs + f] += G[k * gs + r];
+                G[k * gs + r] = 0.f;
+            }
+        __syncwarp();
+    }
+    for (int k = 0; k < K; k++) {
+        const int f = dup[k];
+        if (f >= 0)
+            for (int r = lane; r < rows; r += 32) {
+                G[f * gs + r] += G[k * gs + r];
+                G[k * gs + r] = 0.f;
+            }
+        __syncwarp();
+    }
+}
+
+// Repulsion of one batch on the tensor cores (BF16 tables, K <= 48 negatives, rows <= 32).
+// Column chunks of M_in (rows) and M_out (negatives) are staged as BF16 with cp.async;
+// pass 1 accumulates G = M_out M_in^T over all chunks in registers (m16n8k16, FP32 accumulate),
+// then G = alpha * (0 - sigma(G)) through the table, repeated words merged, G rounded to BF16;
+// pass 2 re-stages each chunk and forms M_out + G M_in and M_in + G^T M_out, rounded
+// stochastically into the tables.
+__device__ __noinline__ void repel_mma(const TrainArgs &a, const Layout &Lo, unsigned char *base, const int32_t *bw, int rows,
+                          const int *negs, int K, float alpha, const float *s_exp, float *Gf, int *dup, int lane,
+                          LaneBits &rb) {
+    using T = __nv_bfloat16;
+    T *w_in = static_cast<T *>(a.w_in);
+    T *w_out = static_cast<T *>(a.w_out);
+    const int ld = a.ld;
+    T *sin = reinterpret_cast<T *>(base);                        // kMmaR x kMmaStride
+    T *sout = sin + (size_t) kMmaR * kMmaStride;                  // kMmaK x kMmaStride
+    T *Gb = reinterpret_cast<T *>(base + Lo.gb_off);              // kMmaK x kGbStride
+    const int g = lane >> 2, t = lane & 3;
+    const int mt1 = (K + 15) >> 4;        // m-tiles of negatives
+    const int nt1 = (rows + 7) >> 3;      // n-tiles of batch rows (pass 1)
+    const int kr = (rows + 15) >> 4;      // 16-row steps of the batch (pass 2)
+    // zero the staging once: padding rows stay zero for every chunk
+    for (int i = lane; i < (kMmaR + kMmaK) * kMmaStride / 8; i += 32)
+        reinterpret_cast<uint4 *>(sin)[i] = make_uint4(0, 0, 0, 0);
+    __syncwarp();
+    auto stage = [&](int col0) {
+        const int pieces = kMmaCols / 8;  // 16-byte pieces per staged row
+        for (int it = lane; it < (rows + K) * pieces; it += 32) {
+            const int rr = it / pieces, pc = it - rr * pieces;
+            T *dst = rr < rows ? sin + (size_t) rr * kMmaStride + pc * 8 : sout + (size_t) (rr - rows) * kMmaStride + pc * 8;
+            const int col = col0 + pc * 8;
+            if (col < ld) {
+                const T *src = rr < rows ? w_in + (size_t) __ldg(bw + rr) * ld + col : w_out + (size_t) negs[rr - rows] * ld + col;
+                cp_async16(dst, src);
+            } else {
+                *reinterpret_cast<uint4 *>(dst) = make_uint4(0, 0, 0, 0);
+            }
+        }
+        cp_async_commit();
+        cp_async_wait_all();
+        __syncwarp();
+    };
+    // ---- pass 1 ----
+    float acc[3][4][4];
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) acc[i][j][e] = 0.f;
+    for (int col0 = 0; col0 < ld; col0 += kMmaCols) {
+        stage(col0);
+#pragma unroll 1
+        for (int ks = 0; ks < kMmaCols / 16; ks++) {
+            unsigned bfr[4][2];
+#pragma unroll
+            for (int np = 0; np < 2; np++) {  // n-tiles 2np, 2np+1
+                if (2 * np < nt1) {
+                    unsigned r[4];
+                    const int n = np * 16 + (lane & 7) + ((lane >> 4) << 3);
+                    const int k = ks * 16 + ((lane >> 3) & 1) * 8;
+                    ldsm_x4(r, sin + (size_t) n * kMmaStride + k);
+                    bfr[2 * np][0] = r[0];
+                    bfr[2 * np][1] = r[1];
+                    bfr[2 * np + 1][0] = r[2];
+                    bfr[2 * np + 1][1] = r[3];
+                }
+            }
+#pragma unroll
+            for (int mt = 0; mt < 3; mt++) {
+                if (mt < mt1) {
+                    unsigned af[4];
+                    ldsm_x4(af, sout + (size_t) (mt * 16 + (lane & 15)) * kMmaStride + ks * 16 + (lane >> 4) * 8);
+#pragma unroll
+                    for (int nt = 0; nt < 4; nt++)
+                        if (nt < nt1) mma16816(acc[mt][nt], af, bfr[nt][0], bfr[nt][1]);
+                }
+            }
+        }
+        __syncwarp();
+    }
+    // raw dot products into Gf (kMmaK x kMmaR), then sigma / label 0 in a rolled loop
+#pragma unroll
+    for (int mt = 0; mt < 3; mt++)
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+            for (int e = 0; e < 4; e++)
+                if (mt < mt1 && nt < nt1)
+                    Gf[(mt * 16 + g + ((e >> 1) << 3)) * kMmaR + nt * 8 + 2 * t + (e & 1)] = acc[mt][nt][e];
+    __syncwarp();
+#pragma unroll 1
+    for (int i = lane; i < K * kMmaR; i += 32)
+        if ((i & (kMmaR - 1)) < rows) Gf[i] = grad_from_table(Gf[i], 0, alpha, s_exp);
+    __syncwarp();
+    merge_repeats(negs, K, bw, rows, Gf, kMmaR, dup, lane);
+    // G in BF16 with zero padding: rows up to 16*mt1, columns up to 16*kr
+    for (int i = lane; i < kMmaK * kGbStride; i += 32) {
+        const int k = i / kGbStride, r = i - k * kGbStride;
+        Gb[i] = __float2bfloat16_rn((k < K && r < rows) ? Gf[k * kMmaR + r] : 0.f);
+    }
+    __syncwarp();
+    // ---- pass 2 ----
+    for (int col0 = 0; col0 < ld; col0 += kMmaCols) {
+        stage(col0);
+        const int ncols = min(kMmaCols, ld - col0);
+#pragma unroll 1
+        for (int nt = 0; nt < ncols / 8; nt++) {
+            // W_out rows of the negatives: M_out + G M_in
+            float o[3][4];
+#pragma unroll
+            for (int mt = 0; mt < 3; mt++)
+#pragma unroll
+                for (int e = 0; e < 4; e++) o[mt][e] = 0.f;
+#pragma unroll 1
+            for (int ks = 0; ks < kr; ks++) {
+                unsigned b[2];
+                ldsm_x2_t(b, sin + (size_t) (ks * 16 + (lane & 15)) * kMmaStride + nt * 8);
+#pragma unroll
+                for (int mt = 0; mt < 3; mt++)
+                    if (mt < mt1) {
+                        unsigned af[4];
+                        ldsm_x4(af, Gb + (size_t) (mt * 16 + (lane & 15)) * kGbStride + ks * 16 + (lane >> 4) * 8);
+                        mma16816(o[mt], af, b[0], b[1]);
+                    }
+            }
+#pragma unroll
+            for (int mt = 0; mt < 3; mt++)
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int k = mt * 16 + g + 8 * h, j = nt * 8 + 2 * t;
+                    if (mt < mt1 && k < K && dup[k] < 0) {
+                        const float2 old = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(sout + (size_t) k * kMmaStride + j));
+                        const float2 nv = make_float2(old.x + o[mt][2 * h], old.y + o[mt][2 * h + 1]);
+                        *reinterpret_cast<unsigned *>(w_out + (size_t) negs[k] * ld + col0 + j) = pack_sr2(nv, rb.next());
+                    }
+                }
+            // W_in rows of the batch: M_in + G^T M_out
+            float q[2][4];
+#pragma unroll
+            for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+                for (int e = 0; e < 4; e++) q[mt][e] = 0.f;
+#pragma unroll 1
+            for (int ks = 0; ks < mt1; ks++) {
+                unsigned b[2];
+                ldsm_x2_t(b, sout + (size_t) (ks * 16 + (lane & 15)) * kMmaStride + nt * 8);
+#pragma unroll
+                for (int mt = 0; mt < 2; mt++)
+                    if (mt < kr) {
+                        unsigned af[4];
+                        const int kk = ks * 16 + ((lane >> 4) << 3) + (lane & 7);
+                        const int rr = mt * 16 + ((lane >> 3) & 1) * 8;
+                        ldsm_x4_t(af, Gb + (size_t) kk * kGbStride + rr);
+                        mma16816(q[mt], af, b[0], b[1]);
+                    }
+            }
+#pragma unroll
+            for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int r = mt * 16 + g + 8 * h, j = nt * 8 + 2 * t;
+                    if (mt < kr && r < rows && dup[K + r] < 0) {
+                        const float2 old = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(sin + (size_t) r * kMmaStride + j));
+                        const float2 nv = make_float2(old.x + q[mt][2 * h], old.y + q[mt][2 * h + 1]);
+                        *reinterpret_cast<unsigned *>(w_in + (size_t) __ldg(bw + r) * ld + col0 + j) = pack_sr2(nv, rb.next());
+                    }
+                }
+        }
+        __syncwarp();
+    }
+}
+
+// Repulsion of one batch on the CUDA cores (FP32 tables, or shapes beyond the mma path): G is
+// accumulated over column chunks staged as FP32, then a second pass writes the new rows.
+template <bool BF16>
+__device__ __noinline__ void repel_simt(const TrainArgs &a, const Layout &Lo, unsigned char *base, const int32_t *bw, int rows,
+                           const int *negs, int K, float alpha, const float *s_exp, float *G, int *dup, int lane,
+                           LaneBits &rb) {
+    using S = Store<BF16>;
+    using T = typename S::T;
+    T *w_in = static_cast<T *>(a.w_in);
+    T *w_out = static_cast<T *>(a.w_out);
+    const int ld = a.ld, B = a.batch;
+    const int stride = Lo.ch + 4;
+    float *s_in = reinterpret_cast<float *>(base);
+    float *s_out = s_in + (size_t) B * stride;
+    const int c4 = Lo.ch / 4;
+    for (int e = lane; e < K * rows; e += 32) G[e] = 0.f;
+    __syncwarp();
+    auto stage_chunk = [&](int col0) {
+        const int ncol4 = min(c4, (ld - col0 + 3) / 4);
+        for (int rr = 0; rr < rows + K; rr++) {
+            const T *src = rr < rows ? w_in + (size_t) __ldg(bw + rr) * ld : w_out + (size_t) negs[rr - rows] * ld;
+            float *dst = rr < rows ? s_in + (size_t) rr * stride : s_out + (size_t) (rr - rows) * stride;
+            for (int j4 = lane; j4 < c4; j4 += 32)
+                reinterpret_cast<float4 *>(dst)[j4] = j4 < ncol4 ? S::load4(src + col0, j4) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        __syncwarp();
+    };
+    for (int col0 = 0; col0 < ld; col0 += Lo.ch) {
+        stage_chunk(col0);
+        for (int e = lane; e < K * rows; e += 32) {
+            const int k = e / rows, r = e - k * rows;
+            const float4 *po = reinterpret_cast<const float4 *>(s_out + (size_t) k * stride);
+            const float4 *pi = reinterpret_cast<const float4 *>(s_in + (size_t) r * stride);
+            float acc = 0.f;
+            for (int j4 = 0; j4 < c4; j4++) {
+                const float4 u = po[j4], v = pi[j4];
+                acc = fmaf(u.x, v.x, fmaf(u.y, v.y, fmaf(u.z, v.z, fmaf(u.w, v.w, acc))));
+            }
+            G[e] += acc;
+        }
+        __syncwarp();
+    }
+    for (int e = lane; e < K * rows; e += 32) G[e] = grad_from_table(G[e], 0, alpha, s_exp);
+    __syncwarp();
+    merge_repeats(negs, K, bw, rows, G, rows, dup, lane);
+    for (int col0 = 0; col0 < ld; col0 += Lo.ch) {
+        stage_chunk(col0);
+        const int ncol4 = min(c4, (ld - col0 + 3) / 4);
+        for (int k = 0; k < K; k++) {
+            if (dup[k] >= 0) continue;
+            for (int j4 = lane; j4 < ncol4; j4 += 32) {
+                float4 acc = reinterpret_cast<const float4 *>(s_out + (size_t) k * stride)[j4];
+                for (int r = 0; r < rows; r++) {
+                    const float gk = G[k * rows + r];
+                    const float4 v = reinterpret_cast<const float4 *>(s_in + (size_t) r * stride)[j4];
+                    acc = make_float4(fmaf(gk, v.x, acc.x), fmaf(gk, v.y, acc.y), fmaf(gk, v.z, acc.z), fmaf(gk, v.w, acc.w));
+                }
+                S::store4(w_out + (size_t) negs[k] * ld + col0, j4, acc, rb.next());
+            }
+        }
+        for (int r = 0; r < rows; r++) {
+            if (dup[K + r] >= 0) continue;
+            const int word = __ldg(bw + r);
+            for (int j4 = lane; j4 < ncol4; j4 += 32) {
+                float4 acc = reinterpret_cast<const float4 *>(s_in + (size_t) r * stride)[j4];
+                for (int k = 0; k < K; k++) {
+                    const float gk = G[k * rows + r];
+                    const float4 v = reinterpret_cast<const float4 *>(s_out + (size_t) k * stride)[j4];
+                    acc = make_float4(fmaf(gk, v.x, acc.x), fmaf(gk, v.y, acc.y), fmaf(gk, v.z, acc.z), fmaf(gk, v.w, acc.w));
+                }
+                S::store4(w_in + (size_t) word * ld + col0, j4, acc, rb.next());
+            }
+        }
+        __syncwarp();
+    }
+}
+
+template <int NV2, bool BF16, bool SYNC>
 __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs a, int warps) {
     using S = Store<BF16>;
     using T = typename S::T;
@@ -164,19 +506,24 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
     unsigned char *base = smem_raw + up16(1004 * sizeof(float)) + (size_t) wid * Lo.per_warp;
     float *cur = reinterpret_cast<float *>(base);                        // ws x ld FP32 (window)
     T *raw = reinterpret_cast<T *>(base + Lo.raw_off);                    // kRing x ld landing (BF16)
-    float *stage = reinterpret_cast<float *>(base);                      // repulsion chunks (aliases)
     T *tgt = reinterpret_cast<T *>(base + Lo.tgt_off);                    // kRing x ld target landing
-    float *G = reinterpret_cast<float *>(base + Lo.g_off);               // kmax x B
+    float *G = reinterpret_cast<float *>(base + Lo.g_off);
     int *negs = reinterpret_cast<int *>(base + Lo.neg_off);
     int *dup = reinterpret_cast<int *>(base + Lo.dup_off);
     int *slot_word = reinterpret_cast<int *>(base + Lo.meta_off);
     int *slot_alias = slot_word + Lo.ws;
+    float *ctx_g = reinterpret_cast<float *>(base + Lo.ctx_off);        // 2w: window-synchronous gradients
+    int *ctx_s = reinterpret_cast<int *>(ctx_g + 2 * w);                 // 2w: and context slots
     int *recent_exit = reinterpret_cast<int *>(base + Lo.exit_off);      // words written back lately
 
     T *w_in = static_cast<T *>(a.w_in);
     T *w_out = static_cast<T *>(a.w_out);
     const uint64_t n_lines = a.cnt->n_lines, total_kept = a.cnt->total_kept;
     const int row_chunks = ld / S::kChunkElems;  // 16-byte pieces per stored row
+    const bool use_mma = Lo.mma;
+    // c mod ws for positions c < 2^16 by a multiply-high reciprocal (exact: ws <= 256)
+    const unsigned ws_u = (unsigned) Lo.ws, ws_m = (unsigned) (0xFFFFFFFFULL / ws_u) + 1u;
+    auto ring = [&](int c) { return (int) ((unsigned) c - __umulhi((unsigned) c, ws_m) * ws_u); };
     unsigned long long st_kept = 0, st_sent = 0, st_pairs = 0, st_batches = 0, st_negs = 0;
     bool failed = false;
 
@@ -191,21 +538,22 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
             const int L = (int) min((uint32_t) kMaxSentence, hi_line - c0);
             const int32_t *sen = a.packed + c0;
             uint64_t rng = sentence_seed_b(a, line, piece);
+            LaneBits rb{mix64(rng ^ (0xA24BAED4963EE407ULL * (uint64_t) (lane + 1))) | 1ULL};
             const float alpha = sentence_alpha_b(a, c0, total_kept);
 
             auto slot_of = [&](int c) {
-                const int s = c % Lo.ws;
+                const int s = ring(c);
                 const int al = slot_alias[s];
                 return al < 0 ? s : al;
             };
             // a position joins the window: share the row with an occurrence already inside, else
             // take the landed copy (BF16: widen it into the slot)
             auto enter = [&](int q, int first_in_window, bool landed_in_slot, const T *landing) {
-                const int s = q % Lo.ws;
+                const int s = ring(q);
                 const int word = __ldg(sen + q);
                 int owner = -1;
                 for (int c = first_in_window + lane; c < q; c += 32) {
-                    const int sc = c % Lo.ws;
+                    const int sc = ring(c);
                     if (slot_alias[sc] < 0 && slot_word[sc] == word) owner = sc;
                 }
                 const unsigned m = __ballot_sync(0xffffffffu, owner >= 0);
@@ -222,7 +570,7 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
                     __syncwarp();
                     if (lane == 0) slot_alias[owner] = s;
                 } else if (!landed_in_slot || recently_written) {
-                    // landed copy may predate this sentence's own write-back of the word: reload
+                    // the landed copy may predate this sentence's own write-back of the word: reload
                     const T *src = (recently_written || landing == nullptr) ? w_in + (size_t) word * ld : landing;
                     for (int qq = lane; qq < n2; qq += 32) reinterpret_cast<float2 *>(dst)[qq] = S::load2(src, qq);
                 }
@@ -232,14 +580,14 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
                 }
                 __syncwarp();
             };
-            auto leave = [&](int q, uint64_t salt) {
-                const int s = q % Lo.ws;
+            auto leave = [&](int q) {
+                const int s = ring(q);
                 if (slot_alias[s] < 0) {
                     const int word = slot_word[s];
                     T *row = w_in + (size_t) word * ld;
                     const float *src = cur + (size_t) s * ld;
                     for (int qq = lane; qq < n2; qq += 32)
-                        S::store2(row, qq, reinterpret_cast<const float2 *>(src)[qq], mix64(salt ^ ((uint64_t) word << 20 | qq)));
+                        S::store2(row, qq, reinterpret_cast<const float2 *>(src)[qq], rb.next());
                     if (lane == 0) {
                         for (int i = kPrefetch - 1; i > 0; i--) recent_exit[i] = recent_exit[i - 1];
                         recent_exit[0] = word;
@@ -256,7 +604,7 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
                 if (qi < L) {
                     const T *src = w_in + (size_t) __ldg(sen + qi) * ld;
                     unsigned char *dst = BF16 ? reinterpret_cast<unsigned char *>(raw + (size_t) (qi % kRing) * ld)
-                                              : reinterpret_cast<unsigned char *>(cur + (size_t) (qi % Lo.ws) * ld);
+                                              : reinterpret_cast<unsigned char *>(cur + (size_t) ring(qi) * ld);
                     for (int m = lane; m < row_chunks; m += 32)
                         cp_async16(dst + 16 * (size_t) m, reinterpret_cast<const unsigned char *>(src) + 16 * (size_t) m);
                 }
@@ -282,7 +630,7 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
             Row<NV2> y;
             int prev_t = -1, prev2_t = -1;
             for (int p = 0; p < L; p++) {
-                if (p - w - 1 >= 0) leave(p - w - 1, rng ^ (uint64_t) p);
+                if (p - w - 1 >= 0) leave(p - w - 1);
                 issue(p + w + kPrefetch, p + kPrefetch);
                 cp_async_wait_prefetch();
                 __syncwarp();
@@ -300,60 +648,121 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
                     }
                 }
                 rng = lcg_next(rng);
-                const int b = (int) (rng % (uint64_t) w);
-                for (int i = b; i < 2 * w + 1 - b; i++) {
-                    if (i == w) continue;
-                    const int c = p - w + i;
-                    if (c < 0) continue;
-                    if (c >= L) break;
-                    float2 *x = reinterpret_cast<float2 *>(cur + (size_t) slot_of(c) * ld);
-                    Row<NV2> xr;
-                    float f = 0.f;
+                const int b = (int) mod_small(rng, (uint32_t) w);
+                if constexpr (SYNC) {
+                    // contexts [p-w+b, p+w-b] \ {p} within the sentence, scored against the same y
+                    const int lo_c = max(p - w + b, 0), hi_c = min(p + w - b, L - 1);
+                    const int n = hi_c - lo_c;  // p itself is inside [lo_c, hi_c]
+                    for (int i0 = 0; i0 < n; i0 += 4) {
+                        float f[4];
+                        int sl[4];
 #pragma unroll
-                    for (int k = 0; k < NV2; k++) {
-                        const int qq = lane + 32 * k;
-                        xr.v[k] = qq < n2 ? x[qq] : make_float2(0.f, 0.f);
-                        f = fmaf(xr.v[k].x, y.v[k].x, fmaf(xr.v[k].y, y.v[k].y, f));
-                    }
-                    f = warp_sum(f);
-                    const float g = grad_from_table(f, 1, alpha, s_exp);
+                        for (int u = 0; u < 4; u++) {
+                            f[u] = 0.f;
+                            sl[u] = -1;
+                            if (i0 + u < n) {
+                                const int c = lo_c + i0 + u + (lo_c + i0 + u >= p ? 1 : 0);
+                                sl[u] = slot_of(c);
+                                const float2 *x = reinterpret_cast<const float2 *>(cur + (size_t) sl[u] * ld);
 #pragma unroll
-                    for (int k = 0; k < NV2; k++) {
-                        const int qq = lane + 32 * k;
-                        const float2 xv = xr.v[k], yv = y.v[k];
-                        y.v[k] = make_float2(fmaf(g, xv.x, yv.x), fmaf(g, xv.y, yv.y));
-                        if (qq < n2) x[qq] = make_float2(fmaf(g, yv.x, xv.x), fmaf(g, yv.y, xv.y));
+                                for (int k = 0; k < NV2; k++) {
+                                    const int qq = lane + 32 * k;
+                                    const float2 xv = qq < n2 ? x[qq] : make_float2(0.f, 0.f);
+                                    f[u] = fmaf(xv.x, y.v[k].x, fmaf(xv.y, y.v[k].y, f[u]));
+                                }
+                            }
+                        }
+#pragma unroll
+                        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                            for (int u = 0; u < 4; u++) f[u] += __shfl_xor_sync(0xffffffffu, f[u], o);
+                        if (lane == 0)
+#pragma unroll
+                            for (int u = 0; u < 4; u++)
+                                if (i0 + u < n) {
+                                    ctx_g[i0 + u] = grad_from_table(f[u], 1, alpha, s_exp);
+                                    ctx_s[i0 + u] = sl[u];
+                                }
                     }
-                    st_pairs++;
+                    __syncwarp();
+                    if (lane == 0)  // a word twice among the contexts: one slot, summed gradient
+                        for (int i = 0; i < n; i++)
+                            for (int k = 0; k < i; k++)
+                                if (ctx_s[k] == ctx_s[i]) {
+                                    ctx_g[k] += ctx_g[i];
+                                    ctx_g[i] = 0.f;
+                                    break;
+                                }
+                    __syncwarp();
+                    Row<NV2> dy;
+#pragma unroll
+                    for (int k = 0; k < NV2; k++) dy.v[k] = make_float2(0.f, 0.f);
+                    for (int i = 0; i < n; i++) {
+                        const float g = ctx_g[i];
+                        float2 *x = reinterpret_cast<float2 *>(cur + (size_t) ctx_s[i] * ld);
+#pragma unroll
+                        for (int k = 0; k < NV2; k++) {
+                            const int qq = lane + 32 * k;
+                            if (qq < n2) {
+                                const float2 xv = x[qq], yv = y.v[k];
+                                dy.v[k] = make_float2(fmaf(g, xv.x, dy.v[k].x), fmaf(g, xv.y, dy.v[k].y));
+                                if (g != 0.f) x[qq] = make_float2(fmaf(g, yv.x, xv.x), fmaf(g, yv.y, xv.y));
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int k = 0; k < NV2; k++) y.v[k] = make_float2(y.v[k].x + dy.v[k].x, y.v[k].y + dy.v[k].y);
+                    st_pairs += n;
+                } else {
+                    for (int i = b; i < 2 * w + 1 - b; i++) {
+                        if (i == w) continue;
+                        const int c = p - w + i;
+                        if (c < 0) continue;
+                        if (c >= L) break;
+                        float2 *x = reinterpret_cast<float2 *>(cur + (size_t) slot_of(c) * ld);
+                        Row<NV2> xr;
+                        float f = 0.f;
+#pragma unroll
+                        for (int k = 0; k < NV2; k++) {
+                            const int qq = lane + 32 * k;
+                            xr.v[k] = qq < n2 ? x[qq] : make_float2(0.f, 0.f);
+                            f = fmaf(xr.v[k].x, y.v[k].x, fmaf(xr.v[k].y, y.v[k].y, f));
+                        }
+                        f = warp_sum(f);
+                        const float g = grad_from_table(f, 1, alpha, s_exp);
+#pragma unroll
+                        for (int k = 0; k < NV2; k++) {
+                            const int qq = lane + 32 * k;
+                            const float2 xv = xr.v[k], yv = y.v[k];
+                            y.v[k] = make_float2(fmaf(g, xv.x, yv.x), fmaf(g, xv.y, yv.y));
+                            if (qq < n2) x[qq] = make_float2(fmaf(g, yv.x, xv.x), fmaf(g, yv.y, xv.y));
+                        }
+                        st_pairs++;
+                    }
                 }
                 // target write-back
                 T *trow = w_out + (size_t) t * ld;
-                const uint64_t h0 = mix64(rng ^ ((uint64_t) t << 21));
 #pragma unroll
                 for (int i = 0; i < NV2; i++) {
                     const int qq = lane + 32 * i;
-                    if (qq < n2) S::store2(trow, qq, y.v[i], mix64(h0 + (uint64_t) qq));
+                    if (qq < n2) S::store2(trow, qq, y.v[i], rb.next());
                 }
                 prev2_t = prev_t;
                 prev_t = t;
                 __syncwarp();
             }
-            for (int q = max(0, L - w - 1); q < L; q++) leave(q, rng ^ (uint64_t) (q + 7919));
+            for (int q = max(0, L - w - 1); q < L; q++) leave(q);
             cp_async_wait_all();
             __threadfence_block();
             __syncwarp();
 
             // ---- repulsion (:571-679) ----
             const int num_batch = (L + B - 1) / B;
-            const int stride = Lo.ch + 4;
-            float *s_in = stage;                         // rows x stride
-            float *s_out = stage + (size_t) B * stride;  // K x stride
             for (int nb = 0; nb < num_batch && !failed; nb++) {
                 const int lo_b = nb * B;
                 const int rows = min(B, L - lo_b);
                 rng = lcg_next(rng);
-                const int rep_b = (lo_b <= w - 1 || (L - 1) - lo_b <= w - 1) ? (int) (rng % (uint64_t) w)
-                                                                              : (int) (rng % (uint64_t) (2 * w));
+                const int rep_b = (int) mod_small(rng, (uint32_t) ((lo_b <= w - 1 || (L - 1) - lo_b <= w - 1) ? w : 2 * w));
                 const int K = rep_b * a.negative;
                 if (!warp_draw_negatives(a.table, a.vocab, rng, sen, L, K, negs, lane, a.max_resample)) {
                     failed = true;  // unresolved negatives: leave the batch untouched
@@ -361,108 +770,15 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
                 }
                 st_batches++;
                 st_negs += K;
-                for (int e = lane; e < K * rows; e += 32) G[e] = 0.f;
-                __syncwarp();
-                const int c4 = Lo.ch / 4;
-                auto stage_chunk = [&](int col0) {
-                    const int ncol4 = min(c4, (ld - col0 + 3) / 4);
-                    for (int it = lane; it < (rows + K) * c4; it += 32) {
-                        const int rr = it / c4, j4 = it - rr * c4;
-                        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-                        if (j4 < ncol4) {
-                            const T *src = rr < rows ? w_in + (size_t) __ldg(sen + lo_b + rr) * ld
-                                                     : w_out + (size_t) negs[rr - rows] * ld;
-                            v = S::load4(src + col0, j4);
-                        }
-                        float *dst = rr < rows ? s_in + (size_t) rr * stride : s_out + (size_t) (rr - rows) * stride;
-                        reinterpret_cast<float4 *>(dst)[j4] = v;
+                if (K > 0) {
+                    if constexpr (BF16) {
+                        if (use_mma)
+                            repel_mma(a, Lo, base, sen + lo_b, rows, negs, K, alpha, s_exp, G, dup, lane, rb);
+                        else
+                            repel_simt<true>(a, Lo, base, sen + lo_b, rows, negs, K, alpha, s_exp, G, dup, lane, rb);
+                    } else {
+                        repel_simt<false>(a, Lo, base, sen + lo_b, rows, negs, K, alpha, s_exp, G, dup, lane, rb);
                     }
-                    __syncwarp();
-                };
-                // pass 1: G[k][r] = M_out[k] . M_in[r], chunk by chunk
-                for (int col0 = 0; col0 < ld; col0 += Lo.ch) {
-                    stage_chunk(col0);
-                    for (int e = lane; e < K * rows; e += 32) {
-                        const int k = e / rows, r = e - k * rows;
-                        const float4 *po = reinterpret_cast<const float4 *>(s_out + (size_t) k * stride);
-                        const float4 *pi = reinterpret_cast<const float4 *>(s_in + (size_t) r * stride);
-                        float acc = 0.f;
-                        for (int j4 = 0; j4 < c4; j4++) {
-                            const float4 u = po[j4], v = pi[j4];
-                            acc = fmaf(u.x, v.x, fmaf(u.y, v.y, fmaf(u.z, v.z, fmaf(u.w, v.w, acc))));
-                        }
-                        G[e] += acc;
-                    }
-                    __syncwarp();
-                }
-                for (int e = lane; e < K * rows; e += 32) G[e] = grad_from_table(G[e], 0, alpha, s_exp);
-                __syncwarp();
-                // merge duplicate negatives / rows so that each distinct row is written once
-                for (int k = lane; k < K; k += 32) {
-                    int first = -1;
-                    for (int q = 0; q < k && first < 0; q++)
-                        if (negs[q] == negs[k]) first = q;
-                    dup[k] = first;
-                }
-                for (int r = lane; r < rows; r += 32) {
-                    int first = -1;
-                    const int wr = __ldg(sen + lo_b + r);
-                    for (int q = 0; q < r && first < 0; q++)
-                        if (__ldg(sen + lo_b + q) == wr) first = q;
-                    dup[K + r] = first;
-                }
-                __syncwarp();
-                for (int r = 0; r < rows; r++) {
-                    const int f = dup[K + r];
-                    if (f >= 0)
-                        for (int k = lane; k < K; k += 32) {
-                            G[k * rows + f] += G[k * rows + r];
-                            G[k * rows + r] = 0.f;
-                        }
-                    __syncwarp();
-                }
-                for (int k = 0; k < K; k++) {
-                    const int f = dup[k];
-                    if (f >= 0)
-                        for (int r = lane; r < rows; r += 32) {
-                            G[f * rows + r] += G[k * rows + r];
-                            G[k * rows + r] = 0.f;
-                        }
-                    __syncwarp();
-                }
-                // pass 2: new rows, chunk by chunk, from freshly staged values
-                const uint64_t salt = mix64(rng ^ 0x9E3779B97F4A7C15ULL);
-                for (int col0 = 0; col0 < ld; col0 += Lo.ch) {
-                    stage_chunk(col0);
-                    const int ncol4 = min(c4, (ld - col0 + 3) / 4);
-                    for (int it = lane; it < K * ncol4; it += 32) {
-                        const int k = it / ncol4, j4 = it - k * ncol4;
-                        if (dup[k] >= 0) continue;
-                        float4 acc = reinterpret_cast<const float4 *>(s_out + (size_t) k * stride)[j4];
-                        for (int r = 0; r < rows; r++) {
-                            const float gk = G[k * rows + r];
-                            const float4 v = reinterpret_cast<const float4 *>(s_in + (size_t) r * stride)[j4];
-                            acc = make_float4(fmaf(gk, v.x, acc.x), fmaf(gk, v.y, acc.y), fmaf(gk, v.z, acc.z),
-                                              fmaf(gk, v.w, acc.w));
-                        }
-                        S::store4(w_out + (size_t) negs[k] * ld + col0, j4, acc,
-                                  mix64(salt ^ ((uint64_t) negs[k] << 20) ^ (uint64_t) (col0 + 4 * j4)));
-                    }
-                    for (int it = lane; it < rows * ncol4; it += 32) {
-                        const int r = it / ncol4, j4 = it - r * ncol4;
-                        if (dup[K + r] >= 0) continue;
-                        float4 acc = reinterpret_cast<const float4 *>(s_in + (size_t) r * stride)[j4];
-                        for (int k = 0; k < K; k++) {
-                            const float gk = G[k * rows + r];
-                            const float4 v = reinterpret_cast<const float4 *>(s_out + (size_t) k * stride)[j4];
-                            acc = make_float4(fmaf(gk, v.x, acc.x), fmaf(gk, v.y, acc.y), fmaf(gk, v.z, acc.z),
-                                              fmaf(gk, v.w, acc.w));
-                        }
-                        const int word = __ldg(sen + lo_b + r);
-                        S::store4(w_in + (size_t) word * ld + col0, j4, acc,
-                                  mix64(salt ^ ((uint64_t) word << 21) ^ (uint64_t) (col0 + 4 * j4) ^ 1ULL));
-                    }
-                    __syncwarp();
                 }
                 __threadfence_block();
                 __syncwarp();
@@ -481,15 +797,20 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
     }
 }
 
-template <int NV2, bool BF16>
-cudaError_t launch_nv(const TrainArgs &a, int grid, int warps, cudaStream_t s) {
+template <int NV2, bool BF16, bool SYNC>
+cudaError_t launch_nvs(const TrainArgs &a, int grid, int warps, cudaStream_t s) {
     const Layout Lo = make_layout(a.ld, a.window, a.negative, a.batch, BF16);
     const size_t smem = up16(1004 * sizeof(float)) + (size_t) warps * Lo.per_warp;
-    cudaError_t e = cudaFuncSetAttribute(k_batched_train<NV2, BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_batched_train<NV2, BF16, SYNC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int) smem);
     if (e != cudaSuccess) return e;
-    k_batched_train<NV2, BF16><<<grid, warps * 32, smem, s>>>(a, warps);
+    k_batched_train<NV2, BF16, SYNC><<<grid, warps * 32, smem, s>>>(a, warps);
     return cudaGetLastError();
+}
+
+template <int NV2, bool BF16>
+cudaError_t launch_nv(const TrainArgs &a, int grid, int warps, cudaStream_t s) {
+    return a.sync_window ? launch_nvs<NV2, BF16, true>(a, grid, warps, s) : launch_nvs<NV2, BF16, false>(a, grid, warps, s);
 }
 
 template <bool BF16>

@@ -66,6 +66,8 @@ __global__ void __launch_bounds__(kDetThreads, 1) k_det_train(TrainArgs a, DevTr
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ DetShared st;
     __shared__ int sen[kMaxSentence];
+    __shared__ float s_g[256];   // window-synchronous variant: per-context gradients
+    __shared__ int s_ctx[256];   // and context words
     const int tid = threadIdx.x;
     const int d = a.d, ld = a.ld, w = a.window, B = a.batch;
     const int kmax = 2 * w * a.negative;
@@ -137,6 +139,50 @@ __global__ void __launch_bounds__(kDetThreads, 1) k_det_train(TrainArgs a, DevTr
         const int len = st.len, pos = st.pos, b = st.b;
         const float alpha = st.alpha;
         const int target = sen[pos < len ? pos : 0];
+        if (a.sync_window && len > 0) {
+            // window-synchronous variant: all contexts scored against the same target row
+            float *y = w_out + (size_t) target * ld;
+            int n = 0;
+            for (int i = b; i < 2 * w + 1 - b; i++) {
+                if (i == w) continue;
+                const int c = pos - w + i;
+                if (c < 0) continue;
+                if (c >= len) break;
+                const float *x = w_in + (size_t) sen[c] * ld;
+                for (int j = tid; j < d; j += kDetThreads) prod[j] = __fmul_rn(x[j], y[j]);
+                __syncthreads();
+                if (tid == 0) {
+                    float f = 0.f;
+                    for (int j = 0; j < d; j++) f = __fadd_rn(f, prod[j]);
+                    s_g[n] = grad_from_table(f, 1, alpha, a.exp_table);
+                    s_ctx[n] = sen[c];
+                    a.cnt->pairs++;
+                }
+                n++;
+                __syncthreads();
+            }
+            if (tid == 0)
+                for (int i = 0; i < n; i++)
+                    for (int k = 0; k < i; k++)
+                        if (s_ctx[k] == s_ctx[i]) {
+                            s_g[k] = __fadd_rn(s_g[k], s_g[i]);
+                            s_g[i] = 0.f;
+                            break;
+                        }
+            __syncthreads();
+            for (int j = tid; j < d; j += kDetThreads) {
+                const float yj = y[j];
+                float dy = 0.f;
+                for (int i = 0; i < n; i++) dy = __fadd_rn(dy, __fmul_rn(s_g[i], w_in[(size_t) s_ctx[i] * ld + j]));
+                for (int i = 0; i < n; i++) {
+                    if (s_g[i] == 0.f) continue;
+                    float *xj = w_in + (size_t) s_ctx[i] * ld + j;
+                    *xj = __fadd_rn(*xj, __fmul_rn(s_g[i], yj));
+                }
+                y[j] = __fadd_rn(yj, dy);
+            }
+            __syncthreads();
+        } else
         for (int i = b; i < 2 * w + 1 - b; i++) {
             if (i == w) continue;
             const int c = pos - w + i;

@@ -69,8 +69,9 @@ __device__ __forceinline__ uint64_t sentence_seed(const TrainArgs &a, uint64_t l
     return mix64(mix64(a.seed ^ (0xD1B54A32D192ED03ULL * (uint64_t) (a.epoch + 1))) ^ (line * 1024ULL + piece));
 }
 
-__host__ __device__ __forceinline__ size_t plain_warp_smem(int kmax, int B) {
-    return sizeof(int) * (size_t) (kMaxSentence + 2 * kmax + B) + sizeof(float) * (size_t) kmax * B;
+__host__ __device__ __forceinline__ size_t plain_warp_smem(int kmax, int B, int w) {
+    return sizeof(int) * (size_t) (kMaxSentence + 2 * kmax + B) + sizeof(float) * (size_t) kmax * B +
+           (sizeof(float) + sizeof(int)) * (size_t) (2 * w);
 }
 
 // Duplicate words among the batch's negatives (and among its rows) would write the same row twice;
@@ -119,11 +120,13 @@ __global__ void __launch_bounds__(kPlainWarps * 32) k_plain_train(TrainArgs a, i
     const int n2 = (a.d + 1) >> 1;
     const int kmax = 2 * w * a.negative;
     float *s_exp = reinterpret_cast<float *>(smem_raw);  // 1004
-    unsigned char *warp_base = smem_raw + 1004 * sizeof(float) + (size_t) wid * plain_warp_smem(kmax, B);
+    unsigned char *warp_base = smem_raw + 1004 * sizeof(float) + (size_t) wid * plain_warp_smem(kmax, B, w);
     int *sen = reinterpret_cast<int *>(warp_base);
     int *negs = sen + kMaxSentence;
     int *dup = negs + kmax;  // kmax + B: duplicate marks of negatives, then of batch rows
     float *grad = reinterpret_cast<float *>(dup + kmax + B);
+    float *ctx_g = grad + (size_t) kmax * B;                  // 2w: window-synchronous gradients
+    int *ctx_w = reinterpret_cast<int *>(ctx_g + 2 * w);       // 2w: and context words
     for (int i = threadIdx.x; i <= kExpTableSize; i += blockDim.x) s_exp[i] = a.exp_table[i];
     __syncthreads();
 
@@ -153,10 +156,57 @@ __global__ void __launch_bounds__(kPlainWarps * 32) k_plain_train(TrainArgs a, i
             // ---- attraction (:529-568) ----
             for (int pos = 0; pos < L; pos++) {
                 rng = lcg_next(rng);
-                const int b = (int) (rng % (uint64_t) w);
+                const int b = (int) mod_small(rng, (uint32_t) w);
                 float *y = w_out + (size_t) sen[pos] * ld;
                 RowReg<NV2> yr;
                 load_row(yr, y, n2, lane);
+                if (a.sync_window) {
+                    // all contexts scored against the same target row, then all updates applied
+                    int n = 0;
+                    for (int i = b; i < 2 * w + 1 - b; i++) {
+                        if (i == w) continue;
+                        const int c = pos - w + i;
+                        if (c < 0) continue;
+                        if (c >= L) break;
+                        RowReg<NV2> xr;
+                        load_row(xr, w_in + (size_t) sen[c] * ld, n2, lane);
+                        const float g = grad_from_table(dot_row(xr, yr), 1, alpha, s_exp);
+                        if (lane == 0) {
+                            ctx_g[n] = g;
+                            ctx_w[n] = sen[c];
+                        }
+                        n++;
+                    }
+                    __syncwarp();
+                    if (lane == 0)
+                        for (int i = 0; i < n; i++)
+                            for (int k = 0; k < i; k++)
+                                if (ctx_w[k] == ctx_w[i]) {
+                                    ctx_g[k] += ctx_g[i];
+                                    ctx_g[i] = 0.f;
+                                    break;
+                                }
+                    __syncwarp();
+                    RowReg<NV2> dy;
+#pragma unroll
+                    for (int q = 0; q < NV2; q++) dy.v[q] = make_float2(0.f, 0.f);
+                    for (int i = 0; i < n; i++) {
+                        const float g = ctx_g[i];
+                        float *x = w_in + (size_t) ctx_w[i] * ld;
+                        RowReg<NV2> xr;
+                        load_row(xr, x, n2, lane);
+#pragma unroll
+                        for (int q = 0; q < NV2; q++) {
+                            dy.v[q] = make_float2(fmaf(g, xr.v[q].x, dy.v[q].x), fmaf(g, xr.v[q].y, dy.v[q].y));
+                            xr.v[q] = make_float2(fmaf(g, yr.v[q].x, xr.v[q].x), fmaf(g, yr.v[q].y, xr.v[q].y));
+                        }
+                        if (g != 0.f) store_row(xr, x, n2, lane);
+                    }
+#pragma unroll
+                    for (int q = 0; q < NV2; q++) yr.v[q] = make_float2(yr.v[q].x + dy.v[q].x, yr.v[q].y + dy.v[q].y);
+                    st_pairs += n;
+                    __syncwarp();
+                } else
                 for (int i = b; i < 2 * w + 1 - b; i++) {
                     if (i == w) continue;
                     const int c = pos - w + i;
@@ -184,8 +234,7 @@ __global__ void __launch_bounds__(kPlainWarps * 32) k_plain_train(TrainArgs a, i
                 const int lo_b = nb * B;
                 const int rows = min(B, L - lo_b);
                 rng = lcg_next(rng);
-                const int rep_b = (lo_b <= w - 1 || (L - 1) - lo_b <= w - 1) ? (int) (rng % (uint64_t) w)
-                                                                              : (int) (rng % (uint64_t) (2 * w));
+                const int rep_b = (int) mod_small(rng, (uint32_t) ((lo_b <= w - 1 || (L - 1) - lo_b <= w - 1) ? w : 2 * w));
                 const int K = rep_b * a.negative;
                 if (!warp_draw_negatives(a.table, a.vocab, rng, sen, L, K, negs, lane, a.max_resample)) {
                     failed = true;  // unresolved negatives: leave the batch untouched
@@ -269,7 +318,7 @@ __global__ void __launch_bounds__(kPlainWarps * 32) k_plain_train(TrainArgs a, i
 template <int NV2>
 cudaError_t launch_plain_nv(const TrainArgs &a, int grid, int warps, cudaStream_t s) {
     const int kmax = 2 * a.window * a.negative;
-    const size_t smem = 1004 * sizeof(float) + (size_t) warps * plain_warp_smem(kmax, a.batch);
+    const size_t smem = 1004 * sizeof(float) + (size_t) warps * plain_warp_smem(kmax, a.batch, a.window);
     cudaError_t e = cudaFuncSetAttribute(k_plain_train<NV2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
     if (e != cudaSuccess) return e;
     k_plain_train<NV2><<<grid, warps * 32, smem, s>>>(a, warps);

@@ -121,3 +121,19 @@ def test_memory_cap_is_enforced():
         with pytest.raises(pw.ParW2VError) as e:
             t.set_vocab(np.array([3, 5, 5], np.uint32))  # the 400 MB table does not fit in 64 MB
         assert e.value.status == pw.ERR_OOM
+
+
+def test_det_window_variant_bit_exact_vs_oracle(golden):
+    """The window-synchronous attraction (the BATCHED modes' default) is pinned the same way:
+    DET with PARW2V_ATTRACT_WINDOW equals the oracle's restatement of that variant bit for bit."""
+    V, d = len(golden.counts), int(golden.flags["size"])
+    w_in, w_out = pwo.init_net(V, d)
+    pwo.train(golden.counts, golden.stream, w_in, w_out, sync_window=1, **golden.train_kwargs())
+    with make(golden, attraction=pw.ATTRACT_WINDOW) as t:
+        t.init_weights()
+        t.set_corpus(golden.stream[:-1])
+        t.train()
+        a, b = t.get_weights()
+    assert np.array_equal(bits(a), bits(w_in)) and np.array_equal(bits(b), bits(w_out))
+    # and it is a different trajectory from the reference's sequential attraction
+    assert not np.array_equal(bits(a), bits(golden.win))

@@ -11,10 +11,10 @@ import par_word2vec_b200 as pw
 pytestmark = pytest.mark.gpu
 
 
-def run(golden, mode, **over):
+def run(golden, mode, attraction=pw.ATTRACT_SEQUENTIAL, **over):
     k = golden.train_kwargs()
     k.update(over)
-    with pw.Trainer(mode=mode, seed=3, grid=1, warps_per_cta=1, **k) as t:
+    with pw.Trainer(mode=mode, seed=3, grid=1, warps_per_cta=1, attraction=attraction, **k) as t:
         t.set_vocab(golden.counts)
         t.init_weights()
         t.set_corpus(golden.stream[:-1])
@@ -22,11 +22,12 @@ def run(golden, mode, **over):
         return st, t.get_weights()
 
 
+@pytest.mark.parametrize("attraction", [pw.ATTRACT_SEQUENTIAL, pw.ATTRACT_WINDOW])
 @pytest.mark.parametrize("case", ["text_small", "graph_small", "edge", "d100"])
-def test_batched_fp32_equals_plain_sequentially(golden_cases, case):
+def test_batched_fp32_equals_plain_sequentially(golden_cases, case, attraction):
     g = golden_cases[case]
-    sp, (pi, po) = run(g, pw.MODE_PLAIN)
-    sb, (bi, bo) = run(g, pw.MODE_BATCHED)
+    sp, (pi, po) = run(g, pw.MODE_PLAIN, attraction)
+    sb, (bi, bo) = run(g, pw.MODE_BATCHED, attraction)
     for k in ("kept", "sentences", "pairs", "batches", "negatives"):
         assert sp[k] == sb[k], k
     scale = max(np.abs(pi).max(), np.abs(po).max())
@@ -36,11 +37,14 @@ def test_batched_fp32_equals_plain_sequentially(golden_cases, case):
     assert err_in < 1e-4 and err_out < 1e-4
 
 
+@pytest.mark.parametrize("attraction", [pw.ATTRACT_SEQUENTIAL, pw.ATTRACT_WINDOW])
 @pytest.mark.parametrize("case", ["text_small", "d100"])
-def test_batched_bf16_tracks_plain_sequentially(golden_cases, case):
+def test_batched_bf16_tracks_plain_sequentially(golden_cases, case, attraction):
+    """BF16 tables with stochastic rounding (and, for these shapes, the tensor-core repulsion)
+    stay within a few percent of the FP32 run that makes the same random decisions."""
     g = golden_cases[case]
-    _, (pi, po) = run(g, pw.MODE_PLAIN)
-    _, (bi, bo) = run(g, pw.MODE_BATCHED_BF16)
+    _, (pi, po) = run(g, pw.MODE_PLAIN, attraction)
+    _, (bi, bo) = run(g, pw.MODE_BATCHED_BF16, attraction)
     rel = np.linalg.norm(bi - pi) / np.linalg.norm(pi)
     print(case, "BF16 relative Frobenius error of W_in", rel)
     assert rel < 0.05

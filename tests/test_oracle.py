@@ -62,3 +62,18 @@ def test_planted_mistake_is_caught(golden):
     w_in[1, 0] = np.nextafter(w_in[1, 0], np.float32(1))
     pwo.train(golden.counts, golden.stream, w_in, w_out, **golden.train_kwargs())
     assert not np.array_equal(bits(w_in), bits(golden.win))
+
+
+def test_window_variant_is_deterministic_and_trains(golden_cases):
+    g = golden_cases["d100"]
+    V, d = len(g.counts), int(g.flags["size"])
+    runs = []
+    for _ in range(2):
+        w_in, w_out = pwo.init_net(V, d)
+        tr = pwo.train(g.counts, g.stream, w_in, w_out, sync_window=1, **g.train_kwargs())
+        assert tr["rc"] == 0
+        runs.append((w_in, w_out))
+    assert np.array_equal(bits(runs[0][0]), bits(runs[1][0]))
+    assert np.isfinite(runs[0][0]).all()
+    rel = np.linalg.norm(runs[0][0] - g.win) / np.linalg.norm(g.win)
+    assert 0 < rel < 0.5  # a different trajectory, same scale as the reference's
