@@ -64,10 +64,18 @@ typedef struct {
                         a small corpus is not processed almost all at once from stale weights
                         (0 = 256, negative = no cap) */
     int attraction;  /* PARW2V_ATTRACT_*: how the contexts of one target are applied */
+    int variant;     /* BATCHED modes: PARW2V_VARIANT_* kernel organisation */
 } parw2v_config;
 
+/* Kernel organisation of the BATCHED modes (cfg.variant) */
+#define PARW2V_VARIANT_AUTO 0    /* STREAM */
+#define PARW2V_VARIANT_WINDOW 1  /* the window's W_in rows held in shared memory as FP32 working
+                                    copies, written back once per window exit */
+#define PARW2V_VARIANT_STREAM 2  /* rows read and written in global memory (L1-resident while the
+                                    window reuses them); more sentences in flight per SM */
+
 /* Attraction variants (cfg.attraction) */
-#define PARW2V_ATTRACT_DEFAULT 0    /* SEQUENTIAL in DET/PLAIN, WINDOW in the BATCHED modes */
+#define PARW2V_ATTRACT_DEFAULT 0    /* SEQUENTIAL */
 #define PARW2V_ATTRACT_SEQUENTIAL 1 /* the reference: each context sees the target row as the
                                        previous context left it (cpu.cpp:536-567) */
 #define PARW2V_ATTRACT_WINDOW 2     /* window-synchronous: all contexts of a target are scored

@@ -24,6 +24,7 @@ TABLE_SIZE = 100_000_000
 EXP_TABLE_SIZE = 1000
 
 ATTRACT_DEFAULT, ATTRACT_SEQUENTIAL, ATTRACT_WINDOW = 0, 1, 2
+VARIANT_AUTO, VARIANT_WINDOW, VARIANT_STREAM = 0, 1, 2
 OK, ERR_ARG, ERR_CUDA, ERR_OOM, ERR_CAPACITY, ERR_TIMEOUT, ERR_STATE, ERR_IO, ERR_NODEV = 0, -1, -2, -3, -4, -5, -6, -7, -8
 
 # every symbol include/parw2v.h declares (checked by tests against the built library)
@@ -48,7 +49,8 @@ class Config(ctypes.Structure):
                 ("batch_size", ctypes.c_int), ("iter", ctypes.c_int), ("alpha", ctypes.c_float),
                 ("sample", ctypes.c_float), ("mode", ctypes.c_int), ("device", ctypes.c_int),
                 ("seed", ctypes.c_uint64), ("grid", ctypes.c_int), ("warps_per_cta", ctypes.c_int),
-                ("mem_cap_bytes", ctypes.c_size_t), ("min_rounds", ctypes.c_int), ("attraction", ctypes.c_int)]
+                ("mem_cap_bytes", ctypes.c_size_t), ("min_rounds", ctypes.c_int), ("attraction", ctypes.c_int),
+                ("variant", ctypes.c_int)]
 
 
 class _Stats(ctypes.Structure):
@@ -179,13 +181,14 @@ class Trainer:
     """One training context on one CUDA device (``parw2v_create`` .. ``parw2v_destroy``)."""
 
     def __init__(self, size=100, window=5, negative=5, batch_size=24, iter=5, alpha=0.025, sample=1e-3,
-                 mode=MODE_BATCHED_BF16, device=0, seed=0, grid=0, warps_per_cta=0, mem_cap_bytes=0, min_rounds=0, attraction=0):
+                 mode=MODE_BATCHED_BF16, device=0, seed=0, grid=0, warps_per_cta=0, mem_cap_bytes=0, min_rounds=0, attraction=0,
+                 variant=0):
         self._lib = load_library()
         if isinstance(mode, str):
             mode = MODE_NAMES[mode]
         self.cfg = Config(int(size), int(window), int(negative), int(batch_size), int(iter), float(alpha),
                           float(sample), int(mode), int(device), int(seed), int(grid), int(warps_per_cta),
-                          int(mem_cap_bytes), int(min_rounds), int(attraction))
+                          int(mem_cap_bytes), int(min_rounds), int(attraction), int(variant))
         self._h = ctypes.c_void_p()
         rc = self._lib.parw2v_create(ctypes.byref(self.cfg), ctypes.byref(self._h))
         if rc:

@@ -135,6 +135,8 @@ int parw2v_create(const parw2v_config *cfg, parw2v_ctx **out) {
         k.sample < 0 || k.mode < PARW2V_MODE_DET || k.mode > PARW2V_MODE_BATCHED_BF16 || k.grid < 0 ||
         k.warps_per_cta < 0)
         return fail(nullptr, PARW2V_ERR_ARG, "invalid configuration value");
+    if (k.variant < PARW2V_VARIANT_AUTO || k.variant > PARW2V_VARIANT_STREAM)
+        return fail(nullptr, PARW2V_ERR_ARG, "invalid kernel variant");
     if (k.attraction < PARW2V_ATTRACT_DEFAULT || k.attraction > PARW2V_ATTRACT_WINDOW)
         return fail(nullptr, PARW2V_ERR_ARG, "invalid attraction variant");
     if (k.window > 100 || k.negative > 100 || k.batch_size > 1000)
@@ -517,6 +519,8 @@ static int ensure_packing(parw2v_ctx *c) {
     return PARW2V_OK;
 }
 
+static bool stream_variant(const parw2v_ctx *c) { return c->cfg.variant != PARW2V_VARIANT_WINDOW; }
+
 static int train_hogwild(parw2v_ctx *c, TrainArgs &a, parw2v_stats *st) {
     int rc = ensure_packing(c);
     if (rc) return rc;
@@ -540,7 +544,8 @@ static int train_hogwild(parw2v_ctx *c, TrainArgs &a, parw2v_stats *st) {
         a.scratch_per_warp = per;
     } else {
         size_t per_warp = 0;
-        const int maxw = batched_max_warps(c->ld, c->cfg.window, c->cfg.negative, c->cfg.batch_size, c->bf16, &per_warp);
+        const int maxw = batched_max_warps(c->ld, c->cfg.window, c->cfg.negative, c->cfg.batch_size, c->bf16, &per_warp,
+                                           stream_variant(c));
         if (maxw <= 0) return fail(c, PARW2V_ERR_CAPACITY, "BATCHED mode: rows do not fit in shared memory");
         if (!warps || warps > maxw) warps = maxw;
         if (!grid) grid = sms;
@@ -570,7 +575,7 @@ static int train_hogwild(parw2v_ctx *c, TrainArgs &a, parw2v_stats *st) {
            "packing kernels");
         CK(c, cudaEventRecord(c->ev1, c->stream), "event");
         cudaError_t e = plain ? launch_plain_train(a, grid, warps, c->stream)
-                              : launch_batched_train(a, c->bf16, grid, warps, c->stream);
+                              : launch_batched_train(a, c->bf16, stream_variant(c), grid, warps, c->stream);
         if (e != cudaSuccess) return cuda_fail(c, e, "training kernel launch");
         CK(c, cudaEventRecord(c->ev2, c->stream), "event");
         CK(c, cudaStreamSynchronize(c->stream), "training kernel");
@@ -639,9 +644,7 @@ int parw2v_train(parw2v_ctx *c, parw2v_stats *st) {
     a.line_end = c->d_line_end;
     a.max_resample = 1LL << 20;
     {
-        const bool batched = c->cfg.mode == PARW2V_MODE_BATCHED || c->cfg.mode == PARW2V_MODE_BATCHED_BF16;
-        a.sync_window = c->cfg.attraction == PARW2V_ATTRACT_WINDOW ||
-                        (c->cfg.attraction == PARW2V_ATTRACT_DEFAULT && batched);
+        a.sync_window = c->cfg.attraction == PARW2V_ATTRACT_WINDOW;
     }
     if (c->cfg.mode == PARW2V_MODE_DET) return train_det(c, a, st);
     rc = ensure_packing(c);

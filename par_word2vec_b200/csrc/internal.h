@@ -70,10 +70,10 @@ cudaError_t launch_pack(const TrainArgs &a, int32_t *packed, uint32_t *line_end,
                         uint32_t *tile_zero, uint64_t n_tiles, cudaStream_t s);
 uint64_t pack_tiles(uint64_t n_tokens);
 cudaError_t launch_plain_train(const TrainArgs &a, int grid, int warps_per_cta, cudaStream_t s);
-cudaError_t launch_batched_train(const TrainArgs &a, bool bf16, int grid, int warps_per_cta, cudaStream_t s);
+cudaError_t launch_batched_train(const TrainArgs &a, bool bf16, bool stream, int grid, int warps_per_cta, cudaStream_t s);
 size_t plain_scratch_floats(int ld, int batch, int window, int negative);
 int plain_warps_per_cta(int requested);
-int batched_max_warps(int ld, int window, int negative, int batch, bool bf16, size_t *smem_per_warp);
+int batched_max_warps(int ld, int window, int negative, int batch, bool bf16, size_t *smem_per_warp, bool stream);
 
 // Loss / adjoint / finite differences
 struct LossBatch {

@@ -95,10 +95,17 @@ __host__ __device__ inline Layout make_layout(int ld, int window, int negative, 
     return L;
 }
 
-template <int NV2>
+template <int NV4>
 struct Row {
-    float2 v[NV2];
+    float4 v[NV4];
 };
+
+__device__ __forceinline__ float4 f4_fma(float g, float4 x, float4 y) {  // g * x + y
+    return make_float4(fmaf(g, x.x, y.x), fmaf(g, x.y, y.y), fmaf(g, x.z, y.z), fmaf(g, x.w, y.w));
+}
+__device__ __forceinline__ float f4_dot(float4 x, float4 y, float acc) {
+    return fmaf(x.x, y.x, fmaf(x.y, y.y, fmaf(x.z, y.z, fmaf(x.w, y.w, acc))));
+}
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
     const unsigned s = (unsigned) __cvta_generic_to_shared(smem);
@@ -241,14 +248,15 @@ __device__ __noinline__ void merge_repeats(const int *negs, int K, const int32_t
 }
 
 // Repulsion of one batch on the tensor cores (BF16 tables, K <= 48 negatives, rows <= 32).
-// Column chunks of M_in (rows) and M_out (negatives) are staged as BF16 with cp.async;
-// pass 1 accumulates G = M_out M_in^T over all chunks in registers (m16n8k16, FP32 accumulate),
-// then G = alpha * (0 - sigma(G)) through the table, repeated words merged, G rounded to BF16;
-// pass 2 re-stages each chunk and forms M_out + G M_in and M_in + G^T M_out, rounded
-// stochastically into the tables.
-__device__ __noinline__ void repel_mma(const TrainArgs &a, const Layout &Lo, unsigned char *base, const int32_t *bw, int rows,
-                          const int *negs, int K, float alpha, const float *s_exp, float *Gf, int *dup, int lane,
-                          LaneBits &rb) {
+// Column chunks of M_in (rows) and M_out (negatives) are staged as BF16 with cp.async.
+// Pass 1 accumulates G = M_out M_in^T over all chunks in registers (m16n8k16, FP32 accumulate);
+// G = alpha * (0 - sigma(G)) through the table, repeated words merged, G rounded to BF16.
+// Pass 2 re-stages each chunk, forms M_out + G M_in and M_in + G^T M_out 8 columns at a time,
+// rounds them stochastically into the staged tile in place and stores every distinct row's
+// 16-byte pieces back to the tables.
+__device__ __noinline__ void repel_mma(const TrainArgs &a, const Layout &Lo, unsigned char *base, const int32_t *bw,
+                                       int rows, const int *negs, int K, float alpha, const float *s_exp, float *Gf,
+                                       int *dup, int lane, LaneBits &rb) {
     using T = __nv_bfloat16;
     T *w_in = static_cast<T *>(a.w_in);
     T *w_out = static_cast<T *>(a.w_out);
@@ -260,28 +268,7 @@ __device__ __noinline__ void repel_mma(const TrainArgs &a, const Layout &Lo, uns
     const int mt1 = (K + 15) >> 4;        // m-tiles of negatives
     const int nt1 = (rows + 7) >> 3;      // n-tiles of batch rows (pass 1)
     const int kr = (rows + 15) >> 4;      // 16-row steps of the batch (pass 2)
-    // zero the staging once: padding rows stay zero for every chunk
-    for (int i = lane; i < (kMmaR + kMmaK) * kMmaStride / 8; i += 32)
-        reinterpret_cast<uint4 *>(sin)[i] = make_uint4(0, 0, 0, 0);
-    __syncwarp();
-    auto stage = [&](int col0) {
-        const int pieces = kMmaCols / 8;  // 16-byte pieces per staged row
-        for (int it = lane; it < (rows + K) * pieces; it += 32) {
-            const int rr = it / pieces, pc = it - rr * pieces;
-            T *dst = rr < rows ? sin + (size_t) rr * kMmaStride + pc * 8 : sout + (size_t) (rr - rows) * kMmaStride + pc * 8;
-            const int col = col0 + pc * 8;
-            if (col < ld) {
-                const T *src = rr < rows ? w_in + (size_t) __ldg(bw + rr) * ld + col : w_out + (size_t) negs[rr - rows] * ld + col;
-                cp_async16(dst, src);
-            } else {
-                *reinterpret_cast<uint4 *>(dst) = make_uint4(0, 0, 0, 0);
-            }
-        }
-        cp_async_commit();
-        cp_async_wait_all();
-        __syncwarp();
-    };
-    // ---- pass 1 ----
+    constexpr int kPieces = kMmaCols / 8; // 16-byte pieces per staged row
     float acc[3][4][4];
 #pragma unroll
     for (int i = 0; i < 3; i++)
@@ -289,126 +276,155 @@ __device__ __noinline__ void repel_mma(const TrainArgs &a, const Layout &Lo, uns
         for (int j = 0; j < 4; j++)
 #pragma unroll
             for (int e = 0; e < 4; e++) acc[i][j][e] = 0.f;
-    for (int col0 = 0; col0 < ld; col0 += kMmaCols) {
-        stage(col0);
+    __syncwarp();
 #pragma unroll 1
-        for (int ks = 0; ks < kMmaCols / 16; ks++) {
-            unsigned bfr[4][2];
-#pragma unroll
-            for (int np = 0; np < 2; np++) {  // n-tiles 2np, 2np+1
-                if (2 * np < nt1) {
-                    unsigned r[4];
-                    const int n = np * 16 + (lane & 7) + ((lane >> 4) << 3);
-                    const int k = ks * 16 + ((lane >> 3) & 1) * 8;
-                    ldsm_x4(r, sin + (size_t) n * kMmaStride + k);
-                    bfr[2 * np][0] = r[0];
-                    bfr[2 * np][1] = r[1];
-                    bfr[2 * np + 1][0] = r[2];
-                    bfr[2 * np + 1][1] = r[3];
-                }
-            }
-#pragma unroll
-            for (int mt = 0; mt < 3; mt++) {
-                if (mt < mt1) {
-                    unsigned af[4];
-                    ldsm_x4(af, sout + (size_t) (mt * 16 + (lane & 15)) * kMmaStride + ks * 16 + (lane >> 4) * 8);
-#pragma unroll
-                    for (int nt = 0; nt < 4; nt++)
-                        if (nt < nt1) mma16816(acc[mt][nt], af, bfr[nt][0], bfr[nt][1]);
-                }
-            }
-        }
+    for (int pass = 0; pass < 2; pass++) {
+        // zero the staging: padding rows stay zero for every chunk of the pass (the FP32 G of
+        // pass 1 may share these bytes, see the streamed kernel)
+        for (int i = lane; i < (kMmaR + kMmaK) * kMmaStride / 8; i += 32)
+            reinterpret_cast<uint4 *>(sin)[i] = make_uint4(0, 0, 0, 0);
         __syncwarp();
-    }
-    // raw dot products into Gf (kMmaK x kMmaR), then sigma / label 0 in a rolled loop
-#pragma unroll
-    for (int mt = 0; mt < 3; mt++)
-#pragma unroll
-        for (int nt = 0; nt < 4; nt++)
-#pragma unroll
-            for (int e = 0; e < 4; e++)
-                if (mt < mt1 && nt < nt1)
-                    Gf[(mt * 16 + g + ((e >> 1) << 3)) * kMmaR + nt * 8 + 2 * t + (e & 1)] = acc[mt][nt][e];
-    __syncwarp();
 #pragma unroll 1
-    for (int i = lane; i < K * kMmaR; i += 32)
-        if ((i & (kMmaR - 1)) < rows) Gf[i] = grad_from_table(Gf[i], 0, alpha, s_exp);
-    __syncwarp();
-    merge_repeats(negs, K, bw, rows, Gf, kMmaR, dup, lane);
-    // G in BF16 with zero padding: rows up to 16*mt1, columns up to 16*kr
-    for (int i = lane; i < kMmaK * kGbStride; i += 32) {
-        const int k = i / kGbStride, r = i - k * kGbStride;
-        Gb[i] = __float2bfloat16_rn((k < K && r < rows) ? Gf[k * kMmaR + r] : 0.f);
-    }
-    __syncwarp();
-    // ---- pass 2 ----
-    for (int col0 = 0; col0 < ld; col0 += kMmaCols) {
-        stage(col0);
-        const int ncols = min(kMmaCols, ld - col0);
+        for (int col0 = 0; col0 < ld; col0 += kMmaCols) {
+            // stage columns [col0, col0 + 64) of the batch rows and the negatives' rows
+            for (int it = lane; it < (rows + K) * kPieces; it += 32) {
+                const int rr = it / kPieces, pc = it - rr * kPieces;
+                T *dst = (rr < rows ? sin + (size_t) rr * kMmaStride : sout + (size_t) (rr - rows) * kMmaStride) + pc * 8;
+                const int col = col0 + pc * 8;
+                if (col < ld) {
+                    const T *src = (rr < rows ? w_in + (size_t) __ldg(bw + rr) * ld : w_out + (size_t) negs[rr - rows] * ld) + col;
+                    cp_async16(dst, src);
+                } else {
+                    *reinterpret_cast<uint4 *>(dst) = make_uint4(0, 0, 0, 0);
+                }
+            }
+            cp_async_commit();
+            cp_async_wait_all();
+            __syncwarp();
+            if (pass == 0) {
 #pragma unroll 1
-        for (int nt = 0; nt < ncols / 8; nt++) {
-            // W_out rows of the negatives: M_out + G M_in
-            float o[3][4];
+                for (int ks = 0; ks < kMmaCols / 16; ks++) {
+                    unsigned bfr[4][2];
+#pragma unroll
+                    for (int np = 0; np < 2; np++) {  // n-tiles 2np, 2np+1 in one ldmatrix.x4
+                        unsigned r[4];
+                        const int n = np * 16 + (lane & 7) + ((lane >> 4) << 3);
+                        ldsm_x4(r, sin + (size_t) n * kMmaStride + ks * 16 + ((lane >> 3) & 1) * 8);
+                        bfr[2 * np][0] = r[0];
+                        bfr[2 * np][1] = r[1];
+                        bfr[2 * np + 1][0] = r[2];
+                        bfr[2 * np + 1][1] = r[3];
+                    }
+#pragma unroll
+                    for (int mt = 0; mt < 3; mt++)
+                        if (mt < mt1) {
+                            unsigned af[4];
+                            ldsm_x4(af, sout + (size_t) (mt * 16 + (lane & 15)) * kMmaStride + ks * 16 + (lane >> 4) * 8);
+#pragma unroll
+                            for (int nt = 0; nt < 4; nt++)
+                                if (nt < nt1) mma16816(acc[mt][nt], af, bfr[nt][0], bfr[nt][1]);
+                        }
+                }
+            } else {
+                const int ncols = min(kMmaCols, ld - col0);
+#pragma unroll 1
+                for (int nt = 0; nt < ncols / 8; nt++) {
+                    float o[3][4], q[2][4];
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        o[0][e] = o[1][e] = o[2][e] = 0.f;
+                        q[0][e] = q[1][e] = 0.f;
+                    }
+                    // M_out update: G (K x rows) . M_in (rows x 8 columns)
+#pragma unroll 1
+                    for (int ks = 0; ks < kr; ks++) {
+                        unsigned b[2];
+                        ldsm_x2_t(b, sin + (size_t) (ks * 16 + (lane & 15)) * kMmaStride + nt * 8);
+#pragma unroll
+                        for (int mt = 0; mt < 3; mt++)
+                            if (mt < mt1) {
+                                unsigned af[4];
+                                ldsm_x4(af, Gb + (size_t) (mt * 16 + (lane & 15)) * kGbStride + ks * 16 + (lane >> 4) * 8);
+                                mma16816(o[mt], af, b[0], b[1]);
+                            }
+                    }
+                    // M_in update: G^T (rows x K) . M_out (K x 8 columns)
+#pragma unroll 1
+                    for (int ks = 0; ks < mt1; ks++) {
+                        unsigned b[2];
+                        ldsm_x2_t(b, sout + (size_t) (ks * 16 + (lane & 15)) * kMmaStride + nt * 8);
+#pragma unroll
+                        for (int mt = 0; mt < 2; mt++)
+                            if (mt < kr) {
+                                unsigned af[4];
+                                ldsm_x4_t(af, Gb + (size_t) (ks * 16 + ((lane >> 4) << 3) + (lane & 7)) * kGbStride +
+                                                  mt * 16 + ((lane >> 3) & 1) * 8);
+                                mma16816(q[mt], af, b[0], b[1]);
+                            }
+                    }
+                    // new values = staged + update, rounded stochastically, in place
+                    const int j = nt * 8 + 2 * t;
+#pragma unroll
+                    for (int mt = 0; mt < 3; mt++)
+                        if (mt < mt1) {
+                            const uint64_t bits = rb.next();
+#pragma unroll
+                            for (int h = 0; h < 2; h++) {
+                                __nv_bfloat162 *cell = reinterpret_cast<__nv_bfloat162 *>(sout + (size_t) (mt * 16 + g + 8 * h) * kMmaStride + j);
+                                const float2 old = __bfloat1622float2(*cell);
+                                *reinterpret_cast<unsigned *>(cell) =
+                                    pack_sr2(make_float2(old.x + o[mt][2 * h], old.y + o[mt][2 * h + 1]), bits >> (32 * h));
+                            }
+                        }
+#pragma unroll
+                    for (int mt = 0; mt < 2; mt++)
+                        if (mt < kr) {
+                            const uint64_t bits = rb.next();
+#pragma unroll
+                            for (int h = 0; h < 2; h++) {
+                                __nv_bfloat162 *cell = reinterpret_cast<__nv_bfloat162 *>(sin + (size_t) (mt * 16 + g + 8 * h) * kMmaStride + j);
+                                const float2 old = __bfloat1622float2(*cell);
+                                *reinterpret_cast<unsigned *>(cell) =
+                                    pack_sr2(make_float2(old.x + q[mt][2 * h], old.y + q[mt][2 * h + 1]), bits >> (32 * h));
+                            }
+                        }
+                }
+                __syncwarp();
+                // each distinct row's new chunk back to its table in 16-byte pieces
+                for (int it = lane; it < (rows + K) * kPieces; it += 32) {
+                    const int rr = it / kPieces, pc = it - rr * kPieces;
+                    const int col = col0 + pc * 8;
+                    if (col >= ld || dup[rr < rows ? K + rr : rr - rows] >= 0) continue;
+                    const T *src = (rr < rows ? sin + (size_t) rr * kMmaStride : sout + (size_t) (rr - rows) * kMmaStride) + pc * 8;
+                    T *dst = (rr < rows ? w_in + (size_t) __ldg(bw + rr) * ld : w_out + (size_t) negs[rr - rows] * ld) + col;
+                    *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(src);
+                }
+            }
+            __syncwarp();
+        }
+        if (pass == 0) {
+            // raw dot products into Gf (kMmaK x kMmaR), sigma / label 0, merge repeats, BF16 copy
 #pragma unroll
             for (int mt = 0; mt < 3; mt++)
 #pragma unroll
-                for (int e = 0; e < 4; e++) o[mt][e] = 0.f;
-#pragma unroll 1
-            for (int ks = 0; ks < kr; ks++) {
-                unsigned b[2];
-                ldsm_x2_t(b, sin + (size_t) (ks * 16 + (lane & 15)) * kMmaStride + nt * 8);
+                for (int nt = 0; nt < 4; nt++)
 #pragma unroll
-                for (int mt = 0; mt < 3; mt++)
-                    if (mt < mt1) {
-                        unsigned af[4];
-                        ldsm_x4(af, Gb + (size_t) (mt * 16 + (lane & 15)) * kGbStride + ks * 16 + (lane >> 4) * 8);
-                        mma16816(o[mt], af, b[0], b[1]);
-                    }
+                    for (int e = 0; e < 4; e++)
+                        if (mt < mt1 && nt < nt1)
+                            Gf[(mt * 16 + g + ((e >> 1) << 3)) * kMmaR + nt * 8 + 2 * t + (e & 1)] = acc[mt][nt][e];
+            __syncwarp();
+            for (int i = lane; i < K * kMmaR; i += 32)
+                if ((i & (kMmaR - 1)) < rows) Gf[i] = grad_from_table(Gf[i], 0, alpha, s_exp);
+            __syncwarp();
+            merge_repeats(negs, K, bw, rows, Gf, kMmaR, dup, lane);
+            for (int i = lane; i < kMmaK * (kGbStride / 2); i += 32) {
+                const int k = i / (kGbStride / 2), r = 2 * (i - k * (kGbStride / 2));
+                const float v0 = (k < K && r < rows) ? Gf[k * kMmaR + r] : 0.f;
+                const float v1 = (k < K && r + 1 < rows) ? Gf[k * kMmaR + r + 1] : 0.f;
+                reinterpret_cast<__nv_bfloat162 *>(Gb)[i] = __floats2bfloat162_rn(v0, v1);
             }
-#pragma unroll
-            for (int mt = 0; mt < 3; mt++)
-#pragma unroll
-                for (int h = 0; h < 2; h++) {
-                    const int k = mt * 16 + g + 8 * h, j = nt * 8 + 2 * t;
-                    if (mt < mt1 && k < K && dup[k] < 0) {
-                        const float2 old = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(sout + (size_t) k * kMmaStride + j));
-                        const float2 nv = make_float2(old.x + o[mt][2 * h], old.y + o[mt][2 * h + 1]);
-                        *reinterpret_cast<unsigned *>(w_out + (size_t) negs[k] * ld + col0 + j) = pack_sr2(nv, rb.next());
-                    }
-                }
-            // W_in rows of the batch: M_in + G^T M_out
-            float q[2][4];
-#pragma unroll
-            for (int mt = 0; mt < 2; mt++)
-#pragma unroll
-                for (int e = 0; e < 4; e++) q[mt][e] = 0.f;
-#pragma unroll 1
-            for (int ks = 0; ks < mt1; ks++) {
-                unsigned b[2];
-                ldsm_x2_t(b, sout + (size_t) (ks * 16 + (lane & 15)) * kMmaStride + nt * 8);
-#pragma unroll
-                for (int mt = 0; mt < 2; mt++)
-                    if (mt < kr) {
-                        unsigned af[4];
-                        const int kk = ks * 16 + ((lane >> 4) << 3) + (lane & 7);
-                        const int rr = mt * 16 + ((lane >> 3) & 1) * 8;
-                        ldsm_x4_t(af, Gb + (size_t) kk * kGbStride + rr);
-                        mma16816(q[mt], af, b[0], b[1]);
-                    }
-            }
-#pragma unroll
-            for (int mt = 0; mt < 2; mt++)
-#pragma unroll
-                for (int h = 0; h < 2; h++) {
-                    const int r = mt * 16 + g + 8 * h, j = nt * 8 + 2 * t;
-                    if (mt < kr && r < rows && dup[K + r] < 0) {
-                        const float2 old = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(sin + (size_t) r * kMmaStride + j));
-                        const float2 nv = make_float2(old.x + q[mt][2 * h], old.y + q[mt][2 * h + 1]);
-                        *reinterpret_cast<unsigned *>(w_in + (size_t) __ldg(bw + r) * ld + col0 + j) = pack_sr2(nv, rb.next());
-                    }
-                }
+            __syncwarp();
         }
-        __syncwarp();
     }
 }
 
@@ -489,14 +505,14 @@ __device__ __noinline__ void repel_simt(const TrainArgs &a, const Layout &Lo, un
     }
 }
 
-template <int NV2, bool BF16, bool SYNC>
+template <int NV4, bool BF16, bool SYNC>
 __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs a, int warps) {
     using S = Store<BF16>;
     using T = typename S::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int w = a.window, B = a.batch, ld = a.ld, d = a.d;
-    const int n2 = (d + 1) >> 1;  // float2 chunks that carry data (the padding stays zero)
+    const int n4 = (d + 3) >> 2;  // float4 chunks that carry data (the padding stays zero)
     const Layout Lo = make_layout(ld, w, a.negative, B, BF16);
     float *s_exp = reinterpret_cast<float *>(smem_raw);
     for (int i = threadIdx.x; i <= kExpTableSize; i += blockDim.x) s_exp[i] = a.exp_table[i];
@@ -541,144 +557,138 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
             LaneBits rb{mix64(rng ^ (0xA24BAED4963EE407ULL * (uint64_t) (lane + 1))) | 1ULL};
             const float alpha = sentence_alpha_b(a, c0, total_kept);
 
-            auto slot_of = [&](int c) {
-                const int s = ring(c);
-                const int al = slot_alias[s];
-                return al < 0 ? s : al;
-            };
-            // a position joins the window: share the row with an occurrence already inside, else
-            // take the landed copy (BF16: widen it into the slot)
-            auto enter = [&](int q, int first_in_window, bool landed_in_slot, const T *landing) {
-                const int s = ring(q);
-                const int word = __ldg(sen + q);
-                int owner = -1;
-                for (int c = first_in_window + lane; c < q; c += 32) {
-                    const int sc = ring(c);
-                    if (slot_alias[sc] < 0 && slot_word[sc] == word) owner = sc;
-                }
-                const unsigned m = __ballot_sync(0xffffffffu, owner >= 0);
-                bool recently_written = false;
-                for (int i = 0; i < kPrefetch; i++) recently_written |= (recent_exit[i] == word);
-                float *dst = cur + (size_t) s * ld;
-                if (m) {
-                    owner = __shfl_sync(0xffffffffu, owner, __ffs(m) - 1);
-                    const float *src = cur + (size_t) owner * ld;
-                    for (int qq = lane; qq < n2; qq += 32)
-                        reinterpret_cast<float2 *>(dst)[qq] = reinterpret_cast<const float2 *>(src)[qq];
-                    for (int i = lane; i < Lo.ws; i += 32)
-                        if (slot_alias[i] == owner) slot_alias[i] = s;
-                    __syncwarp();
-                    if (lane == 0) slot_alias[owner] = s;
-                } else if (!landed_in_slot || recently_written) {
-                    // the landed copy may predate this sentence's own write-back of the word: reload
-                    const T *src = (recently_written || landing == nullptr) ? w_in + (size_t) word * ld : landing;
-                    for (int qq = lane; qq < n2; qq += 32) reinterpret_cast<float2 *>(dst)[qq] = S::load2(src, qq);
-                }
-                if (lane == 0) {
-                    slot_word[s] = word;
-                    slot_alias[s] = -1;
-                }
-                __syncwarp();
-            };
-            auto leave = [&](int q) {
-                const int s = ring(q);
-                if (slot_alias[s] < 0) {
-                    const int word = slot_word[s];
-                    T *row = w_in + (size_t) word * ld;
-                    const float *src = cur + (size_t) s * ld;
-                    for (int qq = lane; qq < n2; qq += 32)
-                        S::store2(row, qq, reinterpret_cast<const float2 *>(src)[qq], rb.next());
-                    if (lane == 0) {
-                        for (int i = kPrefetch - 1; i > 0; i--) recent_exit[i] = recent_exit[i - 1];
-                        recent_exit[0] = word;
-                    }
-                }
-                __syncwarp();  // orders this write-back before any lane's later read of the row
-                if (lane == 0) {
-                    slot_word[s] = -1;
-                    slot_alias[s] = -1;
-                }
-                __syncwarp();
-            };
-            auto issue = [&](int qi, int qt) {  // prefetch W_in row of position qi, W_out row of target qt
-                if (qi < L) {
-                    const T *src = w_in + (size_t) __ldg(sen + qi) * ld;
-                    unsigned char *dst = BF16 ? reinterpret_cast<unsigned char *>(raw + (size_t) (qi % kRing) * ld)
-                                              : reinterpret_cast<unsigned char *>(cur + (size_t) ring(qi) * ld);
-                    for (int m = lane; m < row_chunks; m += 32)
-                        cp_async16(dst + 16 * (size_t) m, reinterpret_cast<const unsigned char *>(src) + 16 * (size_t) m);
-                }
-                if (qt < L) {
-                    const T *src = w_out + (size_t) __ldg(sen + qt) * ld;
-                    unsigned char *dst = reinterpret_cast<unsigned char *>(tgt + (size_t) (qt % kRing) * ld);
-                    for (int m = lane; m < row_chunks; m += 32)
-                        cp_async16(dst + 16 * (size_t) m, reinterpret_cast<const unsigned char *>(src) + 16 * (size_t) m);
-                }
-                cp_async_commit();
-            };
-
-            // ---- attraction ----
+            // ---- attraction (:529-568) ----
+            // One loop from p = -max(w, P) to L + w: positions join the window at step q - w (the
+            // first max(w, P) of them synchronously, the rest from P-ahead cp.async copies), the
+            // target of step p >= 0 is trained, and position q leaves at step q + w + 1.
             for (int i = lane; i < Lo.ws; i += 32) {
                 slot_word[i] = -1;
                 slot_alias[i] = -1;
             }
             if (lane < kPrefetch) recent_exit[lane] = -1;
             __syncwarp();
-            const int pro = min(w, L);
-            for (int q = 0; q < pro; q++) enter(q, 0, false, nullptr);  // synchronous loads
-            for (int s = 0; s < kPrefetch; s++) issue(w + s, s);
-            Row<NV2> y;
+            Row<NV4> y;
             int prev_t = -1, prev2_t = -1;
-            for (int p = 0; p < L; p++) {
-                if (p - w - 1 >= 0) leave(p - w - 1);
-                issue(p + w + kPrefetch, p + kPrefetch);
-                cp_async_wait_prefetch();
+            const int p_first = -max(w, kPrefetch);
+            for (int p = p_first; p <= L + w; p++) {
+                // leave: the row of position p - w - 1 goes back to the table once its last
+                // occurrence in the window is done (overwrite; BF16 rounds stochastically)
+                const int q_out = p - w - 1;
+                if (q_out >= 0 && q_out < L) {
+                    const int s = ring(q_out);
+                    if (slot_alias[s] < 0) {
+                        const int word = slot_word[s];
+                        T *row = w_in + (size_t) word * ld;
+                        const float4 *src = reinterpret_cast<const float4 *>(cur + (size_t) s * ld);
+                        for (int c = lane; c < n4; c += 32) S::store4(row, c, src[c], rb.next());
+                        if (lane == 0) {
+                            for (int i = kPrefetch - 1; i > 0; i--) recent_exit[i] = recent_exit[i - 1];
+                            recent_exit[0] = word;
+                        }
+                    }
+                    __syncwarp();
+                    if (lane == 0) {
+                        slot_word[s] = -1;
+                        slot_alias[s] = -1;
+                    }
+                }
+                if (p >= L) continue;
+                // prefetch: W_in row of position p + w + P, W_out row of target p + P
+                if (p >= -kPrefetch) {
+                    const int qi = p + w + kPrefetch, qt = p + kPrefetch;
+                    if (qi < L) {
+                        const unsigned char *src = reinterpret_cast<const unsigned char *>(w_in + (size_t) __ldg(sen + qi) * ld);
+                        unsigned char *dst = BF16 ? reinterpret_cast<unsigned char *>(raw + (size_t) (qi % kRing) * ld)
+                                                  : reinterpret_cast<unsigned char *>(cur + (size_t) ring(qi) * ld);
+                        for (int m = lane; m < row_chunks; m += 32) cp_async16(dst + 16 * (size_t) m, src + 16 * (size_t) m);
+                    }
+                    if (qt >= 0 && qt < L) {
+                        const unsigned char *src = reinterpret_cast<const unsigned char *>(w_out + (size_t) __ldg(sen + qt) * ld);
+                        unsigned char *dst = reinterpret_cast<unsigned char *>(tgt + (size_t) (qt % kRing) * ld);
+                        for (int m = lane; m < row_chunks; m += 32) cp_async16(dst + 16 * (size_t) m, src + 16 * (size_t) m);
+                    }
+                    cp_async_commit();
+                }
+                if (p >= 0) cp_async_wait_prefetch();
                 __syncwarp();
+                // enter: position p + w joins the window; a word already inside keeps one shared
+                // copy (ownership moves to the newest occurrence)
                 const int qn = p + w;
-                if (qn < L && qn >= pro)
-                    enter(qn, max(0, p - w), !BF16, BF16 ? raw + (size_t) (qn % kRing) * ld : nullptr);
-                // target row into registers
+                if (qn >= 0 && qn < L) {
+                    const int s = ring(qn);
+                    const int word = __ldg(sen + qn);
+                    int owner = -1;
+                    for (int c = max(0, p - w) + lane; c < qn; c += 32) {
+                        const int sc = ring(c);
+                        if (slot_alias[sc] < 0 && slot_word[sc] == word) owner = sc;
+                    }
+                    const unsigned m = __ballot_sync(0xffffffffu, owner >= 0);
+                    bool recently_written = false;
+                    for (int i = 0; i < kPrefetch; i++) recently_written |= (recent_exit[i] == word);
+                    float4 *dst = reinterpret_cast<float4 *>(cur + (size_t) s * ld);
+                    const bool landed = qn >= w;  // prefetched (else loaded here)
+                    if (m) {
+                        owner = __shfl_sync(0xffffffffu, owner, __ffs(m) - 1);
+                        const float4 *src = reinterpret_cast<const float4 *>(cur + (size_t) owner * ld);
+                        for (int c = lane; c < n4; c += 32) dst[c] = src[c];
+                        for (int i = lane; i < Lo.ws; i += 32)
+                            if (slot_alias[i] == owner) slot_alias[i] = s;
+                        __syncwarp();
+                        if (lane == 0) slot_alias[owner] = s;
+                    } else if (BF16 || !landed || recently_written) {
+                        // a landed copy can predate this sentence's own write-back of the word: reload
+                        const T *src = (recently_written || !landed) ? w_in + (size_t) word * ld
+                                                                     : raw + (size_t) (qn % kRing) * ld;
+                        for (int c = lane; c < n4; c += 32) dst[c] = S::load4(src, c);
+                    }
+                    if (lane == 0) {
+                        slot_word[s] = word;
+                        slot_alias[s] = -1;
+                    }
+                    __syncwarp();
+                }
+                if (p < 0) continue;
+                // the target row into registers (reused when the word repeats; reloaded when its
+                // landed copy predates the write-back two positions ago)
                 const int t = __ldg(sen + p);
                 if (t != prev_t) {
                     const T *src = (t == prev2_t) ? w_out + (size_t) t * ld : tgt + (size_t) (p % kRing) * ld;
 #pragma unroll
-                    for (int i = 0; i < NV2; i++) {
-                        const int qq = lane + 32 * i;
-                        y.v[i] = qq < n2 ? S::load2(src, qq) : make_float2(0.f, 0.f);
+                    for (int i = 0; i < NV4; i++) {
+                        const int c = lane + 32 * i;
+                        y.v[i] = c < n4 ? S::load4(src, c) : make_float4(0.f, 0.f, 0.f, 0.f);
                     }
                 }
                 rng = lcg_next(rng);
                 const int b = (int) mod_small(rng, (uint32_t) w);
+                const int lo_c = max(p - w + b, 0), hi_c = min(p + w - b, L - 1);
+                const int n = hi_c - lo_c;  // contexts [lo_c, hi_c] without p, in window order
                 if constexpr (SYNC) {
-                    // contexts [p-w+b, p+w-b] \ {p} within the sentence, scored against the same y
-                    const int lo_c = max(p - w + b, 0), hi_c = min(p + w - b, L - 1);
-                    const int n = hi_c - lo_c;  // p itself is inside [lo_c, hi_c]
-                    for (int i0 = 0; i0 < n; i0 += 4) {
-                        float f[4];
-                        int sl[4];
+                    // window-synchronous: every context scored against the same target row
+                    for (int i0 = 0; i0 < n; i0 += 2) {
+                        float f[2] = {0.f, 0.f};
+                        int sl[2] = {-1, -1};
 #pragma unroll
-                        for (int u = 0; u < 4; u++) {
-                            f[u] = 0.f;
-                            sl[u] = -1;
+                        for (int u = 0; u < 2; u++)
                             if (i0 + u < n) {
                                 const int c = lo_c + i0 + u + (lo_c + i0 + u >= p ? 1 : 0);
-                                sl[u] = slot_of(c);
-                                const float2 *x = reinterpret_cast<const float2 *>(cur + (size_t) sl[u] * ld);
+                                const int s0 = ring(c), al = slot_alias[s0];
+                                sl[u] = al < 0 ? s0 : al;
+                                const float4 *x = reinterpret_cast<const float4 *>(cur + (size_t) sl[u] * ld);
 #pragma unroll
-                                for (int k = 0; k < NV2; k++) {
-                                    const int qq = lane + 32 * k;
-                                    const float2 xv = qq < n2 ? x[qq] : make_float2(0.f, 0.f);
-                                    f[u] = fmaf(xv.x, y.v[k].x, fmaf(xv.y, y.v[k].y, f[u]));
+                                for (int k = 0; k < NV4; k++) {
+                                    const int cc = lane + 32 * k;
+                                    if (cc < n4) f[u] = f4_dot(x[cc], y.v[k], f[u]);
                                 }
                             }
+#pragma unroll
+                        for (int o = 16; o > 0; o >>= 1) {
+                            f[0] += __shfl_xor_sync(0xffffffffu, f[0], o);
+                            f[1] += __shfl_xor_sync(0xffffffffu, f[1], o);
                         }
-#pragma unroll
-                        for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-                            for (int u = 0; u < 4; u++) f[u] += __shfl_xor_sync(0xffffffffu, f[u], o);
                         if (lane == 0)
 #pragma unroll
-                            for (int u = 0; u < 4; u++)
+                            for (int u = 0; u < 2; u++)
                                 if (i0 + u < n) {
                                     ctx_g[i0 + u] = grad_from_table(f[u], 1, alpha, s_exp);
                                     ctx_s[i0 + u] = sl[u];
@@ -686,7 +696,7 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
                     }
                     __syncwarp();
                     if (lane == 0)  // a word twice among the contexts: one slot, summed gradient
-                        for (int i = 0; i < n; i++)
+                        for (int i = 1; i < n; i++)
                             for (int k = 0; k < i; k++)
                                 if (ctx_s[k] == ctx_s[i]) {
                                     ctx_g[k] += ctx_g[i];
@@ -694,64 +704,63 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
                                     break;
                                 }
                     __syncwarp();
-                    Row<NV2> dy;
+                    Row<NV4> dy;
 #pragma unroll
-                    for (int k = 0; k < NV2; k++) dy.v[k] = make_float2(0.f, 0.f);
+                    for (int k = 0; k < NV4; k++) dy.v[k] = make_float4(0.f, 0.f, 0.f, 0.f);
                     for (int i = 0; i < n; i++) {
                         const float g = ctx_g[i];
-                        float2 *x = reinterpret_cast<float2 *>(cur + (size_t) ctx_s[i] * ld);
+                        float4 *x = reinterpret_cast<float4 *>(cur + (size_t) ctx_s[i] * ld);
 #pragma unroll
-                        for (int k = 0; k < NV2; k++) {
-                            const int qq = lane + 32 * k;
-                            if (qq < n2) {
-                                const float2 xv = x[qq], yv = y.v[k];
-                                dy.v[k] = make_float2(fmaf(g, xv.x, dy.v[k].x), fmaf(g, xv.y, dy.v[k].y));
-                                if (g != 0.f) x[qq] = make_float2(fmaf(g, yv.x, xv.x), fmaf(g, yv.y, xv.y));
+                        for (int k = 0; k < NV4; k++) {
+                            const int cc = lane + 32 * k;
+                            if (cc < n4) {
+                                const float4 xv = x[cc];
+                                dy.v[k] = f4_fma(g, xv, dy.v[k]);
+                                if (g != 0.f) x[cc] = f4_fma(g, y.v[k], xv);
                             }
                         }
                     }
 #pragma unroll
-                    for (int k = 0; k < NV2; k++) y.v[k] = make_float2(y.v[k].x + dy.v[k].x, y.v[k].y + dy.v[k].y);
-                    st_pairs += n;
+                    for (int k = 0; k < NV4; k++)
+                        y.v[k] = make_float4(y.v[k].x + dy.v[k].x, y.v[k].y + dy.v[k].y, y.v[k].z + dy.v[k].z,
+                                             y.v[k].w + dy.v[k].w);
                 } else {
-                    for (int i = b; i < 2 * w + 1 - b; i++) {
-                        if (i == w) continue;
-                        const int c = p - w + i;
-                        if (c < 0) continue;
-                        if (c >= L) break;
-                        float2 *x = reinterpret_cast<float2 *>(cur + (size_t) slot_of(c) * ld);
-                        Row<NV2> xr;
+                    // the reference's order: each context sees the target row as the previous left it
+                    for (int i = 0; i < n; i++) {
+                        const int c = lo_c + i + (lo_c + i >= p ? 1 : 0);
+                        const int s0 = ring(c), al = slot_alias[s0];
+                        float4 *x = reinterpret_cast<float4 *>(cur + (size_t) (al < 0 ? s0 : al) * ld);
+                        Row<NV4> xr;
                         float f = 0.f;
 #pragma unroll
-                        for (int k = 0; k < NV2; k++) {
-                            const int qq = lane + 32 * k;
-                            xr.v[k] = qq < n2 ? x[qq] : make_float2(0.f, 0.f);
-                            f = fmaf(xr.v[k].x, y.v[k].x, fmaf(xr.v[k].y, y.v[k].y, f));
+                        for (int k = 0; k < NV4; k++) {
+                            const int cc = lane + 32 * k;
+                            xr.v[k] = cc < n4 ? x[cc] : make_float4(0.f, 0.f, 0.f, 0.f);
+                            f = f4_dot(xr.v[k], y.v[k], f);
                         }
                         f = warp_sum(f);
                         const float g = grad_from_table(f, 1, alpha, s_exp);
 #pragma unroll
-                        for (int k = 0; k < NV2; k++) {
-                            const int qq = lane + 32 * k;
-                            const float2 xv = xr.v[k], yv = y.v[k];
-                            y.v[k] = make_float2(fmaf(g, xv.x, yv.x), fmaf(g, xv.y, yv.y));
-                            if (qq < n2) x[qq] = make_float2(fmaf(g, yv.x, xv.x), fmaf(g, yv.y, xv.y));
+                        for (int k = 0; k < NV4; k++) {
+                            const int cc = lane + 32 * k;
+                            const float4 yv = y.v[k];
+                            y.v[k] = f4_fma(g, xr.v[k], yv);
+                            if (cc < n4) x[cc] = f4_fma(g, yv, xr.v[k]);
                         }
-                        st_pairs++;
                     }
                 }
+                st_pairs += n;
                 // target write-back
                 T *trow = w_out + (size_t) t * ld;
 #pragma unroll
-                for (int i = 0; i < NV2; i++) {
-                    const int qq = lane + 32 * i;
-                    if (qq < n2) S::store2(trow, qq, y.v[i], rb.next());
+                for (int i = 0; i < NV4; i++) {
+                    const int c = lane + 32 * i;
+                    if (c < n4) S::store4(trow, c, y.v[i], rb.next());
                 }
                 prev2_t = prev_t;
                 prev_t = t;
                 __syncwarp();
             }
-            for (int q = max(0, L - w - 1); q < L; q++) leave(q);
             cp_async_wait_all();
             __threadfence_block();
             __syncwarp();
@@ -797,49 +806,292 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
     }
 }
 
-template <int NV2, bool BF16, bool SYNC>
+template <int NV4, bool BF16, bool SYNC>
 cudaError_t launch_nvs(const TrainArgs &a, int grid, int warps, cudaStream_t s) {
     const Layout Lo = make_layout(a.ld, a.window, a.negative, a.batch, BF16);
     const size_t smem = up16(1004 * sizeof(float)) + (size_t) warps * Lo.per_warp;
-    cudaError_t e = cudaFuncSetAttribute(k_batched_train<NV2, BF16, SYNC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_batched_train<NV4, BF16, SYNC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int) smem);
     if (e != cudaSuccess) return e;
-    k_batched_train<NV2, BF16, SYNC><<<grid, warps * 32, smem, s>>>(a, warps);
+    k_batched_train<NV4, BF16, SYNC><<<grid, warps * 32, smem, s>>>(a, warps);
     return cudaGetLastError();
 }
 
-template <int NV2, bool BF16>
+template <int NV4, bool BF16>
 cudaError_t launch_nv(const TrainArgs &a, int grid, int warps, cudaStream_t s) {
-    return a.sync_window ? launch_nvs<NV2, BF16, true>(a, grid, warps, s) : launch_nvs<NV2, BF16, false>(a, grid, warps, s);
+    return a.sync_window ? launch_nvs<NV4, BF16, true>(a, grid, warps, s) : launch_nvs<NV4, BF16, false>(a, grid, warps, s);
+}
+
+// ---- STREAM variant: rows stay in global memory (L1-resident while a window reuses them) ----
+// Attraction reads and writes W rows directly, as the PLAIN kernel does, in lanes of 16-byte
+// chunks (BF16 tables rounded stochastically at every write); the repulsion is the same on-chip
+// staged tensor-core (BF16) or CUDA-core (FP32) contraction as the WINDOW variant.  Without the
+// window ring a warp needs ~16 KB of shared memory, so more sentences are in flight per SM.
+constexpr int kMaxWarpsS = 16;
+constexpr size_t kStreamStage = (size_t) (kMmaR + kMmaK) * kMmaStride * 2;  // 11,520 bytes
+
+__host__ __device__ inline Layout make_layout_stream(int ld, int window, int negative, int batch, bool bf16) {
+    Layout L;
+    L.ws = 0;
+    L.kmax = 2 * window * negative;
+    L.mma = mma_path((2 * window - 1) * negative, batch, bf16);
+    L.raw_off = 0;
+    L.tgt_off = 0;
+    L.meta_off = 0;
+    const size_t rows_rep = (size_t) (batch + L.kmax);
+    long ch = (long) (kStreamStage / (rows_rep * 4)) - 4;
+    ch = ch / 4 * 4;
+    if (ch > ((ld + 3) / 4) * 4) ch = ((ld + 3) / 4) * 4;
+    if (ch < 16) ch = 16;
+    L.ch = (int) ch;
+    if (L.mma) {
+        L.gb_off = kStreamStage;
+        L.region = kStreamStage + up16((size_t) kMmaK * kGbStride * 2);
+        L.g_off = 0;  // the FP32 G of pass 1 shares the staging bytes
+    } else {
+        L.gb_off = 0;
+        L.region = up16(rows_rep * (size_t) (L.ch + 4) * 4);
+        L.g_off = L.region;
+    }
+    const size_t g_bytes = L.mma ? 0 : up16((size_t) L.kmax * batch * 4);
+    L.neg_off = L.region + g_bytes;
+    L.dup_off = L.neg_off + up16((size_t) L.kmax * 4);
+    L.ctx_off = L.dup_off + up16((size_t) (L.kmax + batch) * 4);
+    L.exit_off = L.ctx_off + up16((size_t) (2 * window) * 8);
+    L.per_warp = L.exit_off;
+    return L;
+}
+
+template <int NV4, bool BF16, bool SYNC>
+__global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a, int warps) {
+    using S = Store<BF16>;
+    using T = typename S::T;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int w = a.window, B = a.batch, ld = a.ld, d = a.d;
+    const int n4 = (d + 3) >> 2;
+    const Layout Lo = make_layout_stream(ld, w, a.negative, B, BF16);
+    float *s_exp = reinterpret_cast<float *>(smem_raw);
+    for (int i = threadIdx.x; i <= kExpTableSize; i += blockDim.x) s_exp[i] = a.exp_table[i];
+    __syncthreads();
+    if (wid >= warps) return;
+    unsigned char *base = smem_raw + up16(1004 * sizeof(float)) + (size_t) wid * Lo.per_warp;
+    float *G = reinterpret_cast<float *>(base + Lo.g_off);
+    int *negs = reinterpret_cast<int *>(base + Lo.neg_off);
+    int *dup = reinterpret_cast<int *>(base + Lo.dup_off);
+    float *ctx_g = reinterpret_cast<float *>(base + Lo.ctx_off);
+    int *ctx_w = reinterpret_cast<int *>(ctx_g + 2 * w);
+    T *w_in = static_cast<T *>(a.w_in);
+    T *w_out = static_cast<T *>(a.w_out);
+    const uint64_t n_lines = a.cnt->n_lines, total_kept = a.cnt->total_kept;
+    unsigned long long st_kept = 0, st_sent = 0, st_pairs = 0, st_batches = 0, st_negs = 0;
+    bool failed = false;
+
+    for (;;) {
+        unsigned long long line = 0;
+        if (lane == 0) line = atomicAdd(&a.cnt->work, 1ULL);
+        line = __shfl_sync(0xffffffffu, line, 0);
+        if (line >= n_lines || failed) break;
+        const uint32_t lo_line = line ? a.line_end[line - 1] : 0u, hi_line = a.line_end[line];
+        int piece = 0;
+        for (uint32_t c0 = lo_line; c0 < hi_line; c0 += kMaxSentence, piece++) {
+            const int L = (int) min((uint32_t) kMaxSentence, hi_line - c0);
+            const int32_t *sen = a.packed + c0;
+            uint64_t rng = sentence_seed_b(a, line, piece);
+            LaneBits rb{mix64(rng ^ (0xA24BAED4963EE407ULL * (uint64_t) (lane + 1))) | 1ULL};
+            const float alpha = sentence_alpha_b(a, c0, total_kept);
+            // ---- attraction (:529-568) ----
+            for (int p = 0; p < L; p++) {
+                rng = lcg_next(rng);
+                const int b = (int) mod_small(rng, (uint32_t) w);
+                const int t = __ldg(sen + p);
+                T *yrow = w_out + (size_t) t * ld;
+                Row<NV4> y;
+#pragma unroll
+                for (int k = 0; k < NV4; k++) {
+                    const int cc = lane + 32 * k;
+                    y.v[k] = cc < n4 ? S::load4(yrow, cc) : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+                const int lo_c = max(p - w + b, 0), hi_c = min(p + w - b, L - 1);
+                const int n = hi_c - lo_c;
+                if constexpr (SYNC) {
+                    for (int i0 = 0; i0 < n; i0 += 2) {
+                        float f[2] = {0.f, 0.f};
+                        int wd[2] = {-1, -1};
+#pragma unroll
+                        for (int u = 0; u < 2; u++)
+                            if (i0 + u < n) {
+                                const int c = lo_c + i0 + u + (lo_c + i0 + u >= p ? 1 : 0);
+                                wd[u] = __ldg(sen + c);
+                                const T *x = w_in + (size_t) wd[u] * ld;
+#pragma unroll
+                                for (int k = 0; k < NV4; k++) {
+                                    const int cc = lane + 32 * k;
+                                    if (cc < n4) f[u] = f4_dot(S::load4(x, cc), y.v[k], f[u]);
+                                }
+                            }
+#pragma unroll
+                        for (int o = 16; o > 0; o >>= 1) {
+                            f[0] += __shfl_xor_sync(0xffffffffu, f[0], o);
+                            f[1] += __shfl_xor_sync(0xffffffffu, f[1], o);
+                        }
+                        if (lane == 0)
+#pragma unroll
+                            for (int u = 0; u < 2; u++)
+                                if (i0 + u < n) {
+                                    ctx_g[i0 + u] = grad_from_table(f[u], 1, alpha, s_exp);
+                                    ctx_w[i0 + u] = wd[u];
+                                }
+                    }
+                    __syncwarp();
+                    if (lane == 0)
+                        for (int i = 1; i < n; i++)
+                            for (int k = 0; k < i; k++)
+                                if (ctx_w[k] == ctx_w[i]) {
+                                    ctx_g[k] += ctx_g[i];
+                                    ctx_g[i] = 0.f;
+                                    break;
+                                }
+                    __syncwarp();
+                    Row<NV4> dy;
+#pragma unroll
+                    for (int k = 0; k < NV4; k++) dy.v[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    for (int i = 0; i < n; i++) {
+                        const float g = ctx_g[i];
+                        T *x = w_in + (size_t) ctx_w[i] * ld;
+#pragma unroll
+                        for (int k = 0; k < NV4; k++) {
+                            const int cc = lane + 32 * k;
+                            if (cc < n4) {
+                                const float4 xv = S::load4(x, cc);
+                                dy.v[k] = f4_fma(g, xv, dy.v[k]);
+                                if (g != 0.f) S::store4(x, cc, f4_fma(g, y.v[k], xv), rb.next());
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int k = 0; k < NV4; k++)
+                        y.v[k] = make_float4(y.v[k].x + dy.v[k].x, y.v[k].y + dy.v[k].y, y.v[k].z + dy.v[k].z,
+                                             y.v[k].w + dy.v[k].w);
+                } else {
+                    for (int i = 0; i < n; i++) {
+                        const int c = lo_c + i + (lo_c + i >= p ? 1 : 0);
+                        T *x = w_in + (size_t) __ldg(sen + c) * ld;
+                        Row<NV4> xr;
+                        float f = 0.f;
+#pragma unroll
+                        for (int k = 0; k < NV4; k++) {
+                            const int cc = lane + 32 * k;
+                            xr.v[k] = cc < n4 ? S::load4(x, cc) : make_float4(0.f, 0.f, 0.f, 0.f);
+                            f = f4_dot(xr.v[k], y.v[k], f);
+                        }
+                        f = warp_sum(f);
+                        const float g = grad_from_table(f, 1, alpha, s_exp);
+#pragma unroll
+                        for (int k = 0; k < NV4; k++) {
+                            const int cc = lane + 32 * k;
+                            const float4 yv = y.v[k];
+                            y.v[k] = f4_fma(g, xr.v[k], yv);
+                            if (cc < n4) S::store4(x, cc, f4_fma(g, yv, xr.v[k]), rb.next());
+                        }
+                    }
+                }
+                st_pairs += n;
+#pragma unroll
+                for (int k = 0; k < NV4; k++) {
+                    const int cc = lane + 32 * k;
+                    if (cc < n4) S::store4(yrow, cc, y.v[k], rb.next());
+                }
+            }
+            __syncwarp();  // this sentence's row writes before any lane's staging reads
+            // ---- repulsion (:571-679) ----
+            const int num_batch = (L + B - 1) / B;
+            for (int nb = 0; nb < num_batch && !failed; nb++) {
+                const int lo_b = nb * B;
+                const int rows = min(B, L - lo_b);
+                rng = lcg_next(rng);
+                const int rep_b = (int) mod_small(rng, (uint32_t) ((lo_b <= w - 1 || (L - 1) - lo_b <= w - 1) ? w : 2 * w));
+                const int K = rep_b * a.negative;
+                if (!warp_draw_negatives(a.table, a.vocab, rng, sen, L, K, negs, lane, a.max_resample)) {
+                    failed = true;
+                    break;
+                }
+                st_batches++;
+                st_negs += K;
+                if (K > 0) {
+                    if constexpr (BF16) {
+                        if (Lo.mma)
+                            repel_mma(a, Lo, base, sen + lo_b, rows, negs, K, alpha, s_exp, G, dup, lane, rb);
+                        else
+                            repel_simt<true>(a, Lo, base, sen + lo_b, rows, negs, K, alpha, s_exp, G, dup, lane, rb);
+                    } else {
+                        repel_simt<false>(a, Lo, base, sen + lo_b, rows, negs, K, alpha, s_exp, G, dup, lane, rb);
+                    }
+                }
+                __syncwarp();
+            }
+            st_kept += L;
+            st_sent++;
+        }
+    }
+    if (lane == 0) {
+        atomicAdd(&a.cnt->kept, st_kept);
+        atomicAdd(&a.cnt->sentences, st_sent);
+        atomicAdd(&a.cnt->pairs, st_pairs);
+        atomicAdd(&a.cnt->batches, st_batches);
+        atomicAdd(&a.cnt->negatives, st_negs);
+        if (failed) atomicOr(&a.cnt->error, kErrResample);
+    }
+}
+
+template <int NV4, bool BF16, bool SYNC>
+cudaError_t launch_stream_nvs(const TrainArgs &a, int grid, int warps, cudaStream_t s) {
+    const Layout Lo = make_layout_stream(a.ld, a.window, a.negative, a.batch, BF16);
+    const size_t smem = up16(1004 * sizeof(float)) + (size_t) warps * Lo.per_warp;
+    cudaError_t e = cudaFuncSetAttribute(k_stream_train<NV4, BF16, SYNC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    if (e != cudaSuccess) return e;
+    k_stream_train<NV4, BF16, SYNC><<<grid, warps * 32, smem, s>>>(a, warps);
+    return cudaGetLastError();
+}
+
+template <bool BF16>
+cudaError_t launch_stream_mode(const TrainArgs &a, int grid, int warps, cudaStream_t s) {
+    const bool y = a.sync_window;
+    switch ((a.d + 127) / 128) {
+        case 1: return y ? launch_stream_nvs<1, BF16, true>(a, grid, warps, s) : launch_stream_nvs<1, BF16, false>(a, grid, warps, s);
+        case 2: return y ? launch_stream_nvs<2, BF16, true>(a, grid, warps, s) : launch_stream_nvs<2, BF16, false>(a, grid, warps, s);
+        case 3: return y ? launch_stream_nvs<3, BF16, true>(a, grid, warps, s) : launch_stream_nvs<3, BF16, false>(a, grid, warps, s);
+        case 4: return y ? launch_stream_nvs<4, BF16, true>(a, grid, warps, s) : launch_stream_nvs<4, BF16, false>(a, grid, warps, s);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 template <bool BF16>
 cudaError_t launch_mode(const TrainArgs &a, int grid, int warps, cudaStream_t s) {
-    switch ((a.d + 63) / 64) {
+    switch ((a.d + 127) / 128) {  // float4 chunks per lane
         case 1: return launch_nv<1, BF16>(a, grid, warps, s);
         case 2: return launch_nv<2, BF16>(a, grid, warps, s);
         case 3: return launch_nv<3, BF16>(a, grid, warps, s);
         case 4: return launch_nv<4, BF16>(a, grid, warps, s);
-        case 5: return launch_nv<5, BF16>(a, grid, warps, s);
-        case 6: return launch_nv<6, BF16>(a, grid, warps, s);
-        case 7: return launch_nv<7, BF16>(a, grid, warps, s);
-        case 8: return launch_nv<8, BF16>(a, grid, warps, s);
         default: return cudaErrorInvalidValue;
     }
 }
 
 }  // namespace
 
-int batched_max_warps(int ld, int window, int negative, int batch, bool bf16, size_t *per_warp) {
-    const Layout Lo = make_layout(ld, window, negative, batch, bf16);
+int batched_max_warps(int ld, int window, int negative, int batch, bool bf16, size_t *per_warp, bool stream) {
+    const Layout Lo = stream ? make_layout_stream(ld, window, negative, batch, bf16) : make_layout(ld, window, negative, batch, bf16);
     if (per_warp) *per_warp = Lo.per_warp;
     const size_t avail = kSmemBudget - up16(1004 * sizeof(float));
     long w = (long) (avail / Lo.per_warp);
-    if (w > kMaxWarpsB) w = kMaxWarpsB;
+    const long cap = stream ? kMaxWarpsS : kMaxWarpsB;
+    if (w > cap) w = cap;
     return (int) w;
 }
 
-cudaError_t launch_batched_train(const TrainArgs &a, bool bf16, int grid, int warps_per_cta, cudaStream_t s) {
+cudaError_t launch_batched_train(const TrainArgs &a, bool bf16, bool stream, int grid, int warps_per_cta, cudaStream_t s) {
+    if (stream)
+        return bf16 ? launch_stream_mode<true>(a, grid, warps_per_cta, s) : launch_stream_mode<false>(a, grid, warps_per_cta, s);
     return bf16 ? launch_mode<true>(a, grid, warps_per_cta, s) : launch_mode<false>(a, grid, warps_per_cta, s);
 }
 

@@ -60,8 +60,8 @@ def score(run, w_in, w_out):
     return loss, rec
 
 
-def train_mode(run, mode, seed=1):
-    with pw.Trainer(mode=mode, seed=seed, size=FLAGS["size"], window=FLAGS["window"], negative=FLAGS["negative"],
+def train_mode(run, mode, seed=1, variant=0):
+    with pw.Trainer(mode=mode, seed=seed, variant=variant, size=FLAGS["size"], window=FLAGS["window"], negative=FLAGS["negative"],
                     batch_size=FLAGS["batch_size"], iter=FLAGS["iter"], alpha=float(FLAGS["alpha"]),
                     sample=float(FLAGS["sample"])) as t:
         t.set_vocab(run["counts"])
@@ -72,16 +72,19 @@ def train_mode(run, mode, seed=1):
     return st, w_in, w_out
 
 
-@pytest.mark.parametrize("mode", [pw.MODE_PLAIN, pw.MODE_BATCHED, pw.MODE_BATCHED_BF16])
-def test_hogwild_matches_reference_loss_and_recall(text_run, mode):
+@pytest.mark.parametrize("mode,variant", [(pw.MODE_PLAIN, 0), (pw.MODE_BATCHED, pw.VARIANT_WINDOW),
+                                          (pw.MODE_BATCHED, pw.VARIANT_STREAM),
+                                          (pw.MODE_BATCHED_BF16, pw.VARIANT_WINDOW),
+                                          (pw.MODE_BATCHED_BF16, pw.VARIANT_STREAM)])
+def test_hogwild_matches_reference_loss_and_recall(text_run, mode, variant):
     ref_loss, ref_rec = score(text_run, text_run["ref_in"], text_run["ref_out"])
-    st, w_in, w_out = train_mode(text_run, mode)
+    st, w_in, w_out = train_mode(text_run, mode, variant=variant)
     assert np.isfinite(w_in).all() and np.isfinite(w_out).all()
     assert st["words"] == len(text_run["stream"])
     loss, rec = score(text_run, w_in, w_out)
     init_in, init_out = pwo.init_net(text_run["V"], text_run["d"])
     init_loss, _ = score(text_run, init_in, init_out)
-    print(f"mode {mode}: loss {loss:.5f} (ref {ref_loss:.5f}, init {init_loss:.5f}) recall {rec:.4f} (ref {ref_rec:.4f}) "
+    print(f"mode {mode} variant {variant}: loss {loss:.5f} (ref {ref_loss:.5f}, init {init_loss:.5f}) recall {rec:.4f} (ref {ref_rec:.4f}) "
           f"kept {st['kept']} ms {st['kernel_ms']:.1f}")
     assert ref_loss < init_loss  # the evaluation set measures training
     assert abs(loss - ref_loss) <= 0.01 * ref_loss
