@@ -173,6 +173,29 @@ int parw2v_loss_fd(parw2v_ctx *ctx, const int32_t *tgt, const int32_t *ctxw, int
                    const int32_t *neg, int n_neg, int ctx_per_window, const int32_t *matrix,
                    const int32_t *row, const int32_t *col, int n_probes, double h, double *grad);
 
+/* ---- Allocation-free deterministic training (no counterpart in the reference) ----
+ * For callers that cannot let a library allocate device memory: a framework whose caching
+ * allocator owns the GPU's memory, or a service that reserves its memory at start-up and must not
+ * meet an allocation failure later.  It runs the DET-mode training (bit-identical to parw2v_train
+ * in PARW2V_MODE_DET) on device buffers the caller owns and calls no cudaMalloc/cudaFree: its
+ * scratch is a 1 MiB array in the library's static device memory, held by every GPU that loads
+ * the library until the process exits.  Limit: (batch_size + 2*window*negative) * ld * 4 bytes
+ * must fit in that 1 MiB less 256 bytes, else PARW2V_ERR_CAPACITY.
+ *   d_corpus     n_tokens word ids followed by one 0 (the "</s>" sentinel), device memory
+ *   d_table      the 100,000,000-entry unigram table (as parw2v_get_table returns it)
+ *   d_exp_table  the 1001-entry sigma table (as parw2v_get_exp_table returns it)
+ *   d_keep_thr   per word: r = (sample * (float) train_words) / (float) count, sqrtf(r) + r, FP32
+ *   d_w_in/out   vocab_size rows of ld floats, trained in place
+ *   stream       a cudaStream_t (NULL = the default stream); the call returns after the stream
+ *                has finished the training, with stats filled (may be NULL)
+ * cfg.device selects the GPU (made current for the call).  The first call on a device looks up
+ * the array's device address; make that first call before any stream capture.  All calls share
+ * the one array, so calls that overlap on the same GPU race: serialise them. */
+int parw2v_det_train_noalloc(const parw2v_config *cfg, int vocab_size, uint64_t train_words,
+                             const int32_t *d_corpus, uint64_t n_tokens, const int32_t *d_table,
+                             const float *d_exp_table, const float *d_keep_thr, float *d_w_in,
+                             float *d_w_out, int ld, void *stream, parw2v_stats *stats);
+
 /* ---- Host front end (reference-identical text handling; no device needed) ---- */
 
 /* LearnVocabFromTrainFile + SortVocab (cpu.cpp:253-292, :204-226): reads a text corpus

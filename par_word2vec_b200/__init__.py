@@ -35,6 +35,7 @@ EXPORTED = [
     "parw2v_loss", "parw2v_loss_adjoint", "parw2v_loss_fd", "parw2v_vocab_learn", "parw2v_vocab_read",
     "parw2v_vocab_free", "parw2v_vocab_size", "parw2v_vocab_train_words", "parw2v_vocab_counts",
     "parw2v_vocab_word", "parw2v_vocab_save", "parw2v_load_stream", "parw2v_save_model",
+    "parw2v_det_train_noalloc",
 ]
 
 
@@ -96,6 +97,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "parw2v_vocab_save": ([P, ctypes.c_char_p], I),
         "parw2v_load_stream": ([P, ctypes.c_char_p, P, U64, P], I),
         "parw2v_save_model": ([P, P, I, I, ctypes.c_char_p], I),
+        "parw2v_det_train_noalloc": ([P, I, U64, P, U64, P, P, P, P, P, I, P, P], I),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

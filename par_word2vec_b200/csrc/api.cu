@@ -53,6 +53,13 @@ struct parw2v_ctx {
 
 static std::string g_create_error;
 
+namespace parw2v {
+int set_global_error(int code, const char *msg) {
+    g_create_error = msg;
+    return code;
+}
+}  // namespace parw2v
+
 static int fail(parw2v_ctx *c, int code, const std::string &msg) {
     if (c) c->err = msg;
     else g_create_error = msg;

@@ -87,6 +87,8 @@ cudaError_t launch_adjoint(const LossBatch &b, const void *w_in, const void *w_o
 cudaError_t launch_loss_fd(const LossBatch &b, const void *w_in, const void *w_out, bool bf16, int d, int ld,
                            const int32_t *matrix, const int32_t *row, const int32_t *col, int n_probes, double h,
                            double *grad, cudaStream_t s);
+// Records the text parw2v_last_error(NULL) returns; returns code.
+int set_global_error(int code, const char *msg);
 cudaError_t launch_widen_bf16(const __nv_bfloat16 *src, float *dst, size_t n, cudaStream_t s);
 cudaError_t launch_narrow_bf16(const float *src, __nv_bfloat16 *dst, size_t n, cudaStream_t s);
 

@@ -8,6 +8,9 @@
 //   - each repulsion GEMM element sums its inner index in ascending order (the order the
 //     oracle's cblas_sgemm fixes), and scatters of duplicate rows apply in the reference's order.
 // The result is bit-identical to the reference built without FMA contraction.
+#include <cstring>
+#include <mutex>
+
 #include "common.cuh"
 #include "internal.h"
 
@@ -338,3 +341,107 @@ cudaError_t launch_det_train(const TrainArgs &a, const DevTrace &tr, cudaStream_
 }
 
 }  // namespace parw2v
+
+// ---- Allocation-free entry point (parw2v_det_train_noalloc) ----
+// Some callers cannot let a library call cudaMalloc: a framework whose caching allocator owns all
+// device memory, or a service that sizes its device memory once at start-up and must not fail
+// later on an allocation.  This entry point runs the deterministic training kernel on buffers the
+// caller owns; its only scratch (the repulsion staging rows and the counters) lives in the array
+// below, which every GPU that loads this library keeps for the life of the process.
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = 1u << 20;  // 1 MiB: counters + (batch + 2*window*negative) x ld floats
+constexpr size_t kNoAllocCounterBytes = 256;       // DevCounters, rounded up
+static_assert(sizeof(parw2v::DevCounters) <= kNoAllocCounterBytes, "counters must fit their slot");
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[kNoAllocMaxDevices];  // device address of g_noalloc_scratch, per device
+
+}  // namespace
+
+extern "C" int parw2v_det_train_noalloc(const parw2v_config *cfg, int vocab_size, uint64_t train_words,
+                                        const int32_t *d_corpus, uint64_t n_tokens, const int32_t *d_table,
+                                        const float *d_exp_table, const float *d_keep_thr, float *d_w_in,
+                                        float *d_w_out, int ld, void *stream, parw2v_stats *stats) {
+    using namespace parw2v;
+    if (!cfg || !d_corpus || !d_table || !d_exp_table || !d_keep_thr || !d_w_in || !d_w_out)
+        return set_global_error(PARW2V_ERR_ARG, "null argument");
+    const parw2v_config &k = *cfg;
+    if (vocab_size < 2 || k.size < 1 || ld < k.size || k.window < 1 || k.window > 100 || k.negative < 0 ||
+        k.negative > 100 || k.batch_size < 1 || k.batch_size > 1000 || k.iter < 1 || !(k.alpha > 0) || k.sample < 0 ||
+        k.device < 0 || k.device >= kNoAllocMaxDevices)
+        return set_global_error(PARW2V_ERR_ARG, "invalid configuration value");
+    const size_t rows = (size_t) k.batch_size + 2 * (size_t) k.window * k.negative;
+    if (kNoAllocCounterBytes + rows * (size_t) ld * sizeof(float) > kNoAllocScratchBytes)
+        return set_global_error(PARW2V_ERR_CAPACITY,
+                                "(batch_size + 2*window*negative) * ld * 4 bytes exceeds the 1 MiB static scratch");
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess) return set_global_error(PARW2V_ERR_NODEV, "no CUDA device");
+    if (prev != k.device && cudaSetDevice(k.device) != cudaSuccess)
+        return set_global_error(PARW2V_ERR_ARG, "device ordinal out of range");
+    int rc = PARW2V_OK;
+    void *scratch = nullptr;
+    {
+        // set-up, once per device with that device current: the device address of the array
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_addr[k.device]) {
+            void *p = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess) rc = set_global_error(PARW2V_ERR_CUDA, cudaGetErrorString(e));
+            else g_noalloc_addr[k.device] = p;
+        }
+        scratch = g_noalloc_addr[k.device];
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    DevCounters h{};
+    if (rc == PARW2V_OK) {
+        DevCounters *cnt = static_cast<DevCounters *>(scratch);
+        TrainArgs a{};
+        a.corpus = d_corpus;
+        a.n_tokens = n_tokens;
+        a.keep_thr = d_keep_thr;
+        a.table = d_table;
+        a.exp_table = d_exp_table;
+        a.w_in = d_w_in;
+        a.w_out = d_w_out;
+        a.ld = ld;
+        a.d = k.size;
+        a.window = k.window;
+        a.negative = k.negative;
+        a.batch = k.batch_size;
+        a.iter = k.iter;
+        a.vocab = vocab_size;
+        a.alpha0 = k.alpha;
+        a.sample = k.sample;
+        a.train_words = train_words;
+        a.seed = k.seed;
+        a.cnt = cnt;
+        a.scratch = reinterpret_cast<float *>(static_cast<unsigned char *>(scratch) + kNoAllocCounterBytes);
+        a.max_resample = 1LL << 20;
+        a.sync_window = k.attraction == PARW2V_ATTRACT_WINDOW;
+        // the counters start at zero on every call; the staging rows are written before read
+        cudaError_t e = cudaMemsetAsync(cnt, 0, sizeof(DevCounters), s);
+        size_t smem = 0;
+        if (e == cudaSuccess) e = launch_det_train(a, DevTrace{}, s, &smem);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&h, cnt, sizeof(h), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = set_global_error(smem > 200 * 1024 ? PARW2V_ERR_CAPACITY : PARW2V_ERR_CUDA, cudaGetErrorString(e));
+        else if (h.error & kErrResample)
+            rc = set_global_error(PARW2V_ERR_TIMEOUT, "negative resampling exceeded its draw limit");
+    }
+    if (rc == PARW2V_OK && stats) {
+        memset(stats, 0, sizeof(*stats));
+        stats->words = h.words;
+        stats->kept = h.kept;
+        stats->sentences = h.sentences;
+        stats->pairs = h.pairs;
+        stats->batches = h.batches;
+        stats->negatives = h.negatives;
+        stats->final_alpha = h.final_alpha;
+    }
+    if (prev != k.device) cudaSetDevice(prev);
+    return rc;
+}
