@@ -126,6 +126,18 @@ def dist_setup(n):
     return dist, dist.get_rank(), dist.get_world_size()
 
 
+def combine_replicas(torch, dist, words: int, ms: float, device: str = "cpu"):
+    """Independent replicas: words of all ranks over the slowest rank's time."""
+    if not dist:
+        return words, ms
+    t = torch.tensor([float(words), ms], dtype=torch.float64, device=device)
+    w = t[:1].clone()
+    dist.all_reduce(w, op=dist.ReduceOp.SUM)
+    m = t[1:].clone()
+    dist.all_reduce(m, op=dist.ReduceOp.MAX)
+    return int(w.item()), float(m.item())
+
+
 def timed_region(torch, dist, fn, steps):
     """Barrier + synchronize, CUDA events around `steps` calls, synchronize + barrier; max over ranks."""
     if dist:
@@ -140,10 +152,8 @@ def timed_region(torch, dist, fn, steps):
     wall = time.perf_counter() - t0
     ms = max(e0.elapsed_time(e1), wall * 1e3)  # the library calls are synchronous; both agree
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        _, ms = combine_replicas(torch, dist, 0, ms, device="cuda")
         dist.barrier()
-        ms = float(t.item())
     return ms, out
 
 
