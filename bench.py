@@ -55,6 +55,18 @@ def parse():
     return ap.parse_args()
 
 
+def measured_traffic_per_kept_position(mode: str):
+    """DRAM bytes per kept position of the training kernel, from the committed ncu summary."""
+    name = {"batched_bf16": "k_stream_train_bf16_10M_tokens.md"}.get(mode)
+    if not name:
+        return None, None
+    path = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(path):
+        return None, None
+    m = re.search(r"traffic_bytes_per_kept_position:\s*([0-9.]+)", open(path).read())
+    return (float(m.group(1)), "profiles/" + name) if m else (None, None)
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -286,8 +298,12 @@ def main():
     alg_bytes = kept * (4 * bytes_per * d + 4) + negs * (2 * bytes_per * d + 4)
     achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
     peak, peak_src = measured_peaks()
+    tpp, tsrc = measured_traffic_per_kept_position(args.mode)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "kernel": "training kernel", "peak_source": peak_src,
+                "traffic": tpp * kept if tpp else None,
+                "traffic_source": (f"ncu dram__bytes_read+write per kept position ({tsrc}, 10M-token capture) "
+                                   f"x kept positions per launch") if tpp else None,
+                "kernel": "training kernel", "peak_source": peak_src,
                 "alg_bytes_per_launch": alg_bytes, "kernel_ms_per_launch": kernel_ms,
                 "pack_ms_per_launch": sum(s["pack_ms"] for s in stats) / len(stats),
                 "alg_bytes_per_kept_position": alg_bytes / max(kept, 1)}
