@@ -562,13 +562,10 @@ static int train_hogwild(parw2v_ctx *c, TrainArgs &a, parw2v_stats *st) {
     if (min_rounds > 0) {
         const uint64_t cap = std::max<uint64_t>(1, c->n_lines / (uint64_t) min_rounds);
         if ((uint64_t) grid * warps > cap) {
-            if (cap < (uint64_t) sms) {
-                warps = 1;
-                grid = (int) cap;
-            } else {
-                warps = std::max(1, std::min(warps, (int) (cap / (uint64_t) sms)));
-                grid = (int) std::max<uint64_t>(1, cap / (uint64_t) warps);
-            }
+            // spread the capped warps over the SMs, never more CTAs than one wave
+            const int per_sm = (int) std::max<uint64_t>(1, cap / (uint64_t) std::min(grid, sms));
+            warps = std::min(warps, per_sm);
+            grid = (int) std::min<uint64_t>((uint64_t) std::min(grid, sms), std::max<uint64_t>(1, cap / (uint64_t) warps));
         }
     }
     c->last_grid = grid;

@@ -38,8 +38,10 @@ constexpr size_t kSmemBudget = 227 * 1024;
 // Tensor-core repulsion (BF16 mode): shapes and staging geometry
 constexpr int kMmaK = 48;        // negatives per batch handled by the mma path (3 m-tiles)
 constexpr int kMmaR = 32;        // batch rows handled by the mma path (2 m-tiles / 4 n-tiles)
-constexpr int kMmaCols = 64;     // column chunk of the staging
-constexpr int kMmaStride = 72;   // staged row stride in bf16 (144 B: conflict-free ldmatrix rows)
+// The column chunk is narrow on purpose: shared memory and L1 are one 256 KB array per SM, and
+// every byte of staging taken from it is a byte of L1 the streamed kernel's row reuse loses.
+constexpr int kMmaCols = 32;     // column chunk of the staging
+constexpr int kMmaStride = 40;   // staged row stride in bf16 (80 B: conflict-free ldmatrix rows)
 constexpr int kGbStride = 40;    // bf16 G row stride (80 B)
 
 __host__ __device__ inline bool mma_path(int kmax_eff, int batch, bool bf16) {
@@ -176,14 +178,19 @@ __device__ __forceinline__ uint64_t sentence_seed_b(const TrainArgs &a, uint64_t
     return mix64(mix64(a.seed ^ (0xD1B54A32D192ED03ULL * (uint64_t) (a.epoch + 1))) ^ (line * 1024ULL + piece));
 }
 
-// Per-lane stream of random bits for stochastic rounding (xorshift64*, Vigna 2016).
+// Per-lane stream of random bits for stochastic rounding: xorshift32 (Marsaglia 2003); two
+// steps give the four 16-bit fields one float4 write-back needs.
 struct LaneBits {
-    uint64_t s;
+    uint32_t s;
+    __device__ __forceinline__ uint32_t step() {
+        s ^= s << 13;
+        s ^= s >> 17;
+        s ^= s << 5;
+        return s;
+    }
     __device__ __forceinline__ uint64_t next() {
-        s ^= s >> 12;
-        s ^= s << 25;
-        s ^= s >> 27;
-        return s * 0x2545F4914F6CDD1DULL;
+        const uint32_t lo = step();
+        return ((uint64_t) step() << 32) | lo;
     }
 };
 
@@ -286,7 +293,7 @@ __device__ __noinline__ void repel_mma(const TrainArgs &a, const Layout &Lo, uns
         __syncwarp();
 #pragma unroll 1
         for (int col0 = 0; col0 < ld; col0 += kMmaCols) {
-            // stage columns [col0, col0 + 64) of the batch rows and the negatives' rows
+            // stage columns [col0, col0 + kMmaCols) of the batch rows and the negatives' rows
             for (int it = lane; it < (rows + K) * kPieces; it += 32) {
                 const int rr = it / kPieces, pc = it - rr * kPieces;
                 T *dst = (rr < rows ? sin + (size_t) rr * kMmaStride : sout + (size_t) (rr - rows) * kMmaStride) + pc * 8;
@@ -554,7 +561,7 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
             const int L = (int) min((uint32_t) kMaxSentence, hi_line - c0);
             const int32_t *sen = a.packed + c0;
             uint64_t rng = sentence_seed_b(a, line, piece);
-            LaneBits rb{mix64(rng ^ (0xA24BAED4963EE407ULL * (uint64_t) (lane + 1))) | 1ULL};
+            LaneBits rb{(uint32_t) mix64(rng ^ (0xA24BAED4963EE407ULL * (uint64_t) (lane + 1))) | 1u};
             const float alpha = sentence_alpha_b(a, c0, total_kept);
 
             // ---- attraction (:529-568) ----
@@ -826,9 +833,11 @@ cudaError_t launch_nv(const TrainArgs &a, int grid, int warps, cudaStream_t s) {
 // Attraction reads and writes W rows directly, as the PLAIN kernel does, in lanes of 16-byte
 // chunks (BF16 tables rounded stochastically at every write); the repulsion is the same on-chip
 // staged tensor-core (BF16) or CUDA-core (FP32) contraction as the WINDOW variant.  Without the
-// window ring a warp needs ~16 KB of shared memory, so more sentences are in flight per SM.
+// window ring a warp needs ~11 KB of shared memory (d = 300, window 5, 5 negatives), so more
+// sentences are in flight per SM and more of the unified L1 is left to cache rows.
 constexpr int kMaxWarpsS = 16;
-constexpr size_t kStreamStage = (size_t) (kMmaR + kMmaK) * kMmaStride * 2;  // 11,520 bytes
+constexpr size_t kStreamStage = (size_t) (kMmaR + kMmaK) * kMmaStride * 2;  // 6,400 bytes
+static_assert(kStreamStage >= (size_t) kMmaK * kMmaR * 4, "the FP32 G of pass 1 shares the staging bytes");
 
 __host__ __device__ inline Layout make_layout_stream(int ld, int window, int negative, int batch, bool bf16) {
     Layout L;
@@ -898,7 +907,7 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
             const int L = (int) min((uint32_t) kMaxSentence, hi_line - c0);
             const int32_t *sen = a.packed + c0;
             uint64_t rng = sentence_seed_b(a, line, piece);
-            LaneBits rb{mix64(rng ^ (0xA24BAED4963EE407ULL * (uint64_t) (lane + 1))) | 1ULL};
+            LaneBits rb{(uint32_t) mix64(rng ^ (0xA24BAED4963EE407ULL * (uint64_t) (lane + 1))) | 1u};
             const float alpha = sentence_alpha_b(a, c0, total_kept);
             // ---- attraction (:529-568) ----
             for (int p = 0; p < L; p++) {
