@@ -119,14 +119,13 @@ __device__ __forceinline__ void cp_async_wait_prefetch() {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
-// Stochastic rounding FP32 -> BF16: add 16 uniform bits below the kept mantissa, truncate.
-__device__ __forceinline__ unsigned short sr_bf16(float x, unsigned bits16) {
-    unsigned u = __float_as_uint(x);
-    if ((u & 0x7f800000u) != 0x7f800000u) u += bits16 & 0xFFFFu;
-    return (unsigned short) (u >> 16);
-}
+// Stochastic rounding of a pair FP32 -> BF16 with the sm_100a conversion cvt.rs: each element
+// takes 16 random bits (v.x the low half of h, v.y the high half), adds them below the kept
+// mantissa and truncates; Inf and NaN pass through.
 __device__ __forceinline__ unsigned pack_sr2(float2 v, uint64_t h) {
-    return (unsigned) sr_bf16(v.x, (unsigned) h) | ((unsigned) sr_bf16(v.y, (unsigned) (h >> 16)) << 16);
+    unsigned d;
+    asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(v.y), "f"(v.x), "r"((unsigned) h));
+    return d;
 }
 
 template <bool BF16>
@@ -178,15 +177,14 @@ __device__ __forceinline__ uint64_t sentence_seed_b(const TrainArgs &a, uint64_t
     return mix64(mix64(a.seed ^ (0xD1B54A32D192ED03ULL * (uint64_t) (a.epoch + 1))) ^ (line * 1024ULL + piece));
 }
 
-// Per-lane stream of random bits for stochastic rounding: xorshift32 (Marsaglia 2003); two
-// steps give the four 16-bit fields one float4 write-back needs.
+// Per-lane stream of random bits for stochastic rounding: a 32-bit LCG (multiplier 747796405,
+// increment 2891336453) with its high half folded into the low half, so both 16-bit fields of a
+// word carry high-order bits; two steps give the four fields one float4 write-back needs.
 struct LaneBits {
     uint32_t s;
     __device__ __forceinline__ uint32_t step() {
-        s ^= s << 13;
-        s ^= s >> 17;
-        s ^= s << 5;
-        return s;
+        s = s * 747796405u + 2891336453u;
+        return s ^ (s >> 16);
     }
     __device__ __forceinline__ uint64_t next() {
         const uint32_t lo = step();
