@@ -22,9 +22,11 @@
 // sentences in flight, adding updates computed from stale copies of a hot row multiplies its
 // step size and diverges; overwriting loses colliding updates, as the reference's unsynchronised
 // `+=` does.  In BF16 mode the global tables are BF16, working copies and accumulation are FP32,
-// and every write-back rounds stochastically (a counter-based hash supplies the 16 random bits).
+// and every write-back rounds stochastically (per-lane LCG bits, the sm_100a cvt.rs conversion).
 #include "common.cuh"
 #include "internal.h"
+#include "mma.cuh"
+#include "sentence.cuh"
 
 namespace parw2v {
 
@@ -119,15 +121,6 @@ __device__ __forceinline__ void cp_async_wait_prefetch() {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
-// Stochastic rounding of a pair FP32 -> BF16 with the sm_100a conversion cvt.rs: each element
-// takes 16 random bits (v.x the low half of h, v.y the high half), adds them below the kept
-// mantissa and truncates; Inf and NaN pass through.
-__device__ __forceinline__ unsigned pack_sr2(float2 v, uint64_t h) {
-    unsigned d;
-    asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(v.y), "f"(v.x), "r"((unsigned) h));
-    return d;
-}
-
 template <bool BF16>
 struct Store;
 
@@ -165,54 +158,6 @@ struct Store<true> {  // BF16 tables
     }
 };
 
-__device__ __forceinline__ float sentence_alpha_b(const TrainArgs &a, uint64_t kept_before, uint64_t total_kept) {
-    const double done = (double) a.epoch * (double) a.n_tokens +
-                        (total_kept ? (double) kept_before / (double) total_kept : 0.0) * (double) a.n_tokens;
-    float alpha = a.alpha0 * (float) (1.0 - done / ((double) a.iter * (double) a.train_words + 1.0));
-    const float floor_a = a.alpha0 * 0.0001f;
-    return alpha < floor_a ? floor_a : alpha;
-}
-
-__device__ __forceinline__ uint64_t sentence_seed_b(const TrainArgs &a, uint64_t line, int piece) {
-    return mix64(mix64(a.seed ^ (0xD1B54A32D192ED03ULL * (uint64_t) (a.epoch + 1))) ^ (line * 1024ULL + piece));
-}
-
-// Per-lane stream of random bits for stochastic rounding: a 32-bit LCG (multiplier 747796405,
-// increment 2891336453) with its high half folded into the low half, so both 16-bit fields of a
-// word carry high-order bits; two steps give the four fields one float4 write-back needs.
-struct LaneBits {
-    uint32_t s;
-    __device__ __forceinline__ uint32_t step() {
-        s = s * 747796405u + 2891336453u;
-        return s ^ (s >> 16);
-    }
-    __device__ __forceinline__ uint64_t next() {
-        const uint32_t lo = step();
-        return ((uint64_t) step() << 32) | lo;
-    }
-};
-
-__device__ __forceinline__ void ldsm_x4(unsigned (&r)[4], const void *p) {
-    const unsigned a = (unsigned) __cvta_generic_to_shared(p);
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(a));
-}
-__device__ __forceinline__ void ldsm_x4_t(unsigned (&r)[4], const void *p) {
-    const unsigned a = (unsigned) __cvta_generic_to_shared(p);
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(a));
-}
-__device__ __forceinline__ void ldsm_x2_t(unsigned (&r)[2], const void *p) {
-    const unsigned a = (unsigned) __cvta_generic_to_shared(p);
-    asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0,%1}, [%2];" : "=r"(r[0]), "=r"(r[1]) : "r"(a));
-}
-// D += A (16x16 bf16, row) * B (16x8 bf16, col), FP32 accumulate
-__device__ __forceinline__ void mma16816(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
-    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-                 "{%0,%1,%2,%3};"
-                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
 
 // Merge gradient rows of repeated negatives and gradient columns of repeated batch words into
 // their first occurrence (G is K x rows with row stride gs), so each distinct row is written once.

@@ -1,0 +1,57 @@
+// Warp-level tensor-core and BF16 helpers shared by the BATCHED kernels (sm_100a): ldmatrix
+// fragment loads, the m16n8k16 BF16 MMA with FP32 accumulation, stochastic rounding of FP32 pairs
+// to BF16, and the per-lane random bits that rounding draws on.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+
+namespace parw2v {
+
+// Stochastic rounding of a pair FP32 -> BF16 with the sm_100a conversion cvt.rs: each element
+// takes 16 random bits (v.x the low half of h, v.y the high half), adds them below the kept
+// mantissa and truncates; Inf and NaN pass through.
+__device__ __forceinline__ unsigned pack_sr2(float2 v, uint64_t h) {
+    unsigned d;
+    asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(v.y), "f"(v.x), "r"((unsigned) h));
+    return d;
+}
+
+// Per-lane stream of random bits for stochastic rounding: a 32-bit LCG (multiplier 747796405,
+// increment 2891336453) with its high half folded into the low half, so both 16-bit fields of a
+// word carry high-order bits; two steps give the four fields one float4 write-back needs.
+struct LaneBits {
+    uint32_t s;
+    __device__ __forceinline__ uint32_t step() {
+        s = s * 747796405u + 2891336453u;
+        return s ^ (s >> 16);
+    }
+    __device__ __forceinline__ uint64_t next() {
+        const uint32_t lo = step();
+        return ((uint64_t) step() << 32) | lo;
+    }
+};
+
+__device__ __forceinline__ void ldsm_x4(unsigned (&r)[4], const void *p) {
+    const unsigned a = (unsigned) __cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(a));
+}
+__device__ __forceinline__ void ldsm_x4_t(unsigned (&r)[4], const void *p) {
+    const unsigned a = (unsigned) __cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(a));
+}
+__device__ __forceinline__ void ldsm_x2_t(unsigned (&r)[2], const void *p) {
+    const unsigned a = (unsigned) __cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0,%1}, [%2];" : "=r"(r[0]), "=r"(r[1]) : "r"(a));
+}
+// D += A (16x16 bf16, row) * B (16x8 bf16, col), FP32 accumulate
+__device__ __forceinline__ void mma16816(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                 "{%0,%1,%2,%3};"
+                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+}  // namespace parw2v
