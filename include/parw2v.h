@@ -60,9 +60,10 @@ typedef struct {
     int grid;        /* Hogwild modes: persistent CTAs, 0 = one wave of the device */
     int warps_per_cta; /* Hogwild modes: sentences in flight per CTA, 0 = tuned default */
     size_t mem_cap_bytes; /* refuse device allocations beyond this total, 0 = no cap */
-    int min_rounds;  /* Hogwild modes: sentences in flight are capped at lines / min_rounds so that
-                        a small corpus is not processed almost all at once from stale weights
-                        (0 = 256, negative = no cap) */
+    int min_rounds;  /* Hogwild modes: cap on sentences in flight, so that a small corpus is not
+                        processed almost all at once from stale weights.  0 = default:
+                        max(10,000 corpus tokens' worth of lines, lines / 8192); > 0: lines /
+                        min_rounds; < 0: no cap */
     int attraction;  /* PARW2V_ATTRACT_*: how the contexts of one target are applied */
     int variant;     /* BATCHED modes: PARW2V_VARIANT_* kernel organisation */
 } parw2v_config;

@@ -18,6 +18,9 @@
 //              over the chunks forms M_out + G M_in and M_in + G^T M_out and writes each distinct
 //              row once (duplicate negatives / rows are merged into one gradient row first).
 //
+// Rows of the global tables are read at L2 (ld.global.cg or cp.async.cg), never from the SM's L1,
+// which is not coherent with other SMs' writes: a hot row served from a stale L1 line would turn
+// its concurrent updates into lost ones.
 // Write-back is "value + own update" (overwrite), never an atomic add: with thousands of
 // sentences in flight, adding updates computed from stale copies of a hot row multiplies its
 // step size and diverges; overwriting loses colliding updates, as the reference's unsynchronised
@@ -131,6 +134,8 @@ struct Store<false> {  // FP32 tables
     __device__ static float2 load2(const float *row, int q) { return reinterpret_cast<const float2 *>(row)[q]; }
     __device__ static void store2(float *row, int q, float2 v, uint64_t) { reinterpret_cast<float2 *>(row)[q] = v; }
     __device__ static float4 load4(const float *row, int j4) { return reinterpret_cast<const float4 *>(row)[j4]; }
+    // a row of the global tables: read at L2, never from this SM's (non-coherent) L1
+    __device__ static float4 load4g(const float *row, int j4) { return __ldcg(reinterpret_cast<const float4 *>(row) + j4); }
     __device__ static void store4(float *row, int j4, float4 v, uint64_t) { reinterpret_cast<float4 *>(row)[j4] = v; }
 };
 
@@ -144,11 +149,15 @@ struct Store<true> {  // BF16 tables
     __device__ static void store2(__nv_bfloat16 *row, int q, float2 v, uint64_t h) {
         reinterpret_cast<unsigned *>(row)[q] = pack_sr2(v, h);
     }
-    __device__ static float4 load4(const __nv_bfloat16 *row, int j4) {
-        const uint2 u = reinterpret_cast<const uint2 *>(row)[j4];
+    __device__ static float4 widen(uint2 u) {
         const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&u.x));
         const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&u.y));
         return make_float4(a.x, a.y, b.x, b.y);
+    }
+    __device__ static float4 load4(const __nv_bfloat16 *row, int j4) { return widen(reinterpret_cast<const uint2 *>(row)[j4]); }
+    // a row of the global tables: read at L2, never from this SM's (non-coherent) L1
+    __device__ static float4 load4g(const __nv_bfloat16 *row, int j4) {
+        return widen(__ldcg(reinterpret_cast<const uint2 *>(row) + j4));
     }
     __device__ static void store4(__nv_bfloat16 *row, int j4, float4 v, uint64_t h) {
         uint2 u;
@@ -401,7 +410,7 @@ __device__ __noinline__ void repel_simt(const TrainArgs &a, const Layout &Lo, un
             const T *src = rr < rows ? w_in + (size_t) __ldg(bw + rr) * ld : w_out + (size_t) negs[rr - rows] * ld;
             float *dst = rr < rows ? s_in + (size_t) rr * stride : s_out + (size_t) (rr - rows) * stride;
             for (int j4 = lane; j4 < c4; j4 += 32)
-                reinterpret_cast<float4 *>(dst)[j4] = j4 < ncol4 ? S::load4(src + col0, j4) : make_float4(0.f, 0.f, 0.f, 0.f);
+                reinterpret_cast<float4 *>(dst)[j4] = j4 < ncol4 ? S::load4g(src + col0, j4) : make_float4(0.f, 0.f, 0.f, 0.f);
         }
         __syncwarp();
     };
@@ -587,9 +596,13 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
                         if (lane == 0) slot_alias[owner] = s;
                     } else if (BF16 || !landed || recently_written) {
                         // a landed copy can predate this sentence's own write-back of the word: reload
-                        const T *src = (recently_written || !landed) ? w_in + (size_t) word * ld
-                                                                     : raw + (size_t) (qn % kRing) * ld;
-                        for (int c = lane; c < n4; c += 32) dst[c] = S::load4(src, c);
+                        if (recently_written || !landed) {
+                            const T *src = w_in + (size_t) word * ld;
+                            for (int c = lane; c < n4; c += 32) dst[c] = S::load4g(src, c);
+                        } else {
+                            const T *src = raw + (size_t) (qn % kRing) * ld;
+                            for (int c = lane; c < n4; c += 32) dst[c] = S::load4(src, c);
+                        }
                     }
                     if (lane == 0) {
                         slot_word[s] = word;
@@ -602,11 +615,12 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
                 // landed copy predates the write-back two positions ago)
                 const int t = __ldg(sen + p);
                 if (t != prev_t) {
-                    const T *src = (t == prev2_t) ? w_out + (size_t) t * ld : tgt + (size_t) (p % kRing) * ld;
+                    const bool fresh = t == prev2_t;  // global row, else the landed copy in shared memory
+                    const T *src = fresh ? w_out + (size_t) t * ld : tgt + (size_t) (p % kRing) * ld;
 #pragma unroll
                     for (int i = 0; i < NV4; i++) {
                         const int c = lane + 32 * i;
-                        y.v[i] = c < n4 ? S::load4(src, c) : make_float4(0.f, 0.f, 0.f, 0.f);
+                        y.v[i] = c < n4 ? (fresh ? S::load4g(src, c) : S::load4(src, c)) : make_float4(0.f, 0.f, 0.f, 0.f);
                     }
                 }
                 rng = lcg_next(rng);
@@ -862,7 +876,7 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
 #pragma unroll
                 for (int k = 0; k < NV4; k++) {
                     const int cc = lane + 32 * k;
-                    y.v[k] = cc < n4 ? S::load4(yrow, cc) : make_float4(0.f, 0.f, 0.f, 0.f);
+                    y.v[k] = cc < n4 ? S::load4g(yrow, cc) : make_float4(0.f, 0.f, 0.f, 0.f);
                 }
                 const int lo_c = max(p - w + b, 0), hi_c = min(p + w - b, L - 1);
                 const int n = hi_c - lo_c;
@@ -879,7 +893,7 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
 #pragma unroll
                                 for (int k = 0; k < NV4; k++) {
                                     const int cc = lane + 32 * k;
-                                    if (cc < n4) f[u] = f4_dot(S::load4(x, cc), y.v[k], f[u]);
+                                    if (cc < n4) f[u] = f4_dot(S::load4g(x, cc), y.v[k], f[u]);
                                 }
                             }
 #pragma unroll
@@ -915,7 +929,7 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                         for (int k = 0; k < NV4; k++) {
                             const int cc = lane + 32 * k;
                             if (cc < n4) {
-                                const float4 xv = S::load4(x, cc);
+                                const float4 xv = S::load4g(x, cc);
                                 dy.v[k] = f4_fma(g, xv, dy.v[k]);
                                 if (g != 0.f) S::store4(x, cc, f4_fma(g, y.v[k], xv), rb.next());
                             }
@@ -934,7 +948,7 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
 #pragma unroll
                         for (int k = 0; k < NV4; k++) {
                             const int cc = lane + 32 * k;
-                            xr.v[k] = cc < n4 ? S::load4(x, cc) : make_float4(0.f, 0.f, 0.f, 0.f);
+                            xr.v[k] = cc < n4 ? S::load4g(x, cc) : make_float4(0.f, 0.f, 0.f, 0.f);
                             f = f4_dot(xr.v[k], y.v[k], f);
                         }
                         f = warp_sum(f);

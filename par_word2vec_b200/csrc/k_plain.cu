@@ -9,10 +9,12 @@
 //   repulsion   per batch of `batch` positions: rep_b and rep_b * negative shared negatives from
 //               the unigram table, redrawn uniformly while they occur in the sentence; M_in and
 //               M_out are staged in the warp's global workspace, the three products run on the
-//               warp.  Each touched row is written back once as (staged value + this batch's
-//               update), duplicates merged first: concurrent writers of a hot row then lose
-//               updates, as the reference's unsynchronised `+=` does, instead of summing
-//               thousands of updates computed from the same stale value (which diverges).
+//               warp.  Each touched row is written back once, duplicates merged first, as (the
+//               row as it is at write-back + this batch's update): the reference's unsynchronised
+//               `+=` with one row's read-to-write window.
+// Table rows are always read at L2 (ld.global.cg): an SM's L1 is not coherent with other SMs'
+// writes, and at thousands of sentences in flight a hot row served from a stale L1 line turns
+// most of its updates into lost ones (the final loss drifts far from the reference's).
 // Random streams: the sentence's LCG starts from mix64(seed, epoch, line, piece); the learning
 // rate decays linearly with the sentence's position in the corpus (the reference decays with the
 // words processed so far, :443).
@@ -37,6 +39,17 @@ __device__ __forceinline__ void load_row(RowReg<NV2> &r, const float *row, int n
     for (int i = 0; i < NV2; i++) {
         const int q = lane + 32 * i;
         r.v[i] = q < n2 ? p[q] : make_float2(0.f, 0.f);
+    }
+}
+// a row of the global tables: read at L2, never from this SM's (non-coherent) L1, so a row that
+// another SM has written is seen as written, not as this SM cached it earlier
+template <int NV2>
+__device__ __forceinline__ void load_row_g(RowReg<NV2> &r, const float *row, int n2, int lane) {
+    const float2 *p = reinterpret_cast<const float2 *>(row);
+#pragma unroll
+    for (int i = 0; i < NV2; i++) {
+        const int q = lane + 32 * i;
+        r.v[i] = q < n2 ? __ldcg(p + q) : make_float2(0.f, 0.f);
     }
 }
 template <int NV2>
@@ -159,7 +172,7 @@ __global__ void __launch_bounds__(kPlainWarps * 32) k_plain_train(TrainArgs a, i
                 const int b = (int) mod_small(rng, (uint32_t) w);
                 float *y = w_out + (size_t) sen[pos] * ld;
                 RowReg<NV2> yr;
-                load_row(yr, y, n2, lane);
+                load_row_g(yr, y, n2, lane);
                 if (a.sync_window) {
                     // all contexts scored against the same target row, then all updates applied
                     int n = 0;
@@ -169,7 +182,7 @@ __global__ void __launch_bounds__(kPlainWarps * 32) k_plain_train(TrainArgs a, i
                         if (c < 0) continue;
                         if (c >= L) break;
                         RowReg<NV2> xr;
-                        load_row(xr, w_in + (size_t) sen[c] * ld, n2, lane);
+                        load_row_g(xr, w_in + (size_t) sen[c] * ld, n2, lane);
                         const float g = grad_from_table(dot_row(xr, yr), 1, alpha, s_exp);
                         if (lane == 0) {
                             ctx_g[n] = g;
@@ -194,7 +207,7 @@ __global__ void __launch_bounds__(kPlainWarps * 32) k_plain_train(TrainArgs a, i
                         const float g = ctx_g[i];
                         float *x = w_in + (size_t) ctx_w[i] * ld;
                         RowReg<NV2> xr;
-                        load_row(xr, x, n2, lane);
+                        load_row_g(xr, x, n2, lane);
 #pragma unroll
                         for (int q = 0; q < NV2; q++) {
                             dy.v[q] = make_float2(fmaf(g, xr.v[q].x, dy.v[q].x), fmaf(g, xr.v[q].y, dy.v[q].y));
@@ -214,7 +227,7 @@ __global__ void __launch_bounds__(kPlainWarps * 32) k_plain_train(TrainArgs a, i
                     if (c >= L) break;
                     float *x = w_in + (size_t) sen[c] * ld;
                     RowReg<NV2> xr;
-                    load_row(xr, x, n2, lane);
+                    load_row_g(xr, x, n2, lane);
                     const float g = grad_from_table(dot_row(xr, yr), 1, alpha, s_exp);
 #pragma unroll
                     for (int q = 0; q < NV2; q++) {
@@ -246,12 +259,12 @@ __global__ void __launch_bounds__(kPlainWarps * 32) k_plain_train(TrainArgs a, i
                 // stage pre-update copies of the batch rows and the negatives' rows
                 for (int r = 0; r < rows; r++) {
                     RowReg<NV2> t;
-                    load_row(t, w_in + (size_t) sen[lo_b + r] * ld, n2, lane);
+                    load_row_g(t, w_in + (size_t) sen[lo_b + r] * ld, n2, lane);
                     store_row(t, m_in + (size_t) r * ld, n2, lane);
                 }
                 for (int k = 0; k < K; k++) {
                     RowReg<NV2> t;
-                    load_row(t, w_out + (size_t) negs[k] * ld, n2, lane);
+                    load_row_g(t, w_out + (size_t) negs[k] * ld, n2, lane);
                     store_row(t, m_out + (size_t) k * ld, n2, lane);
                 }
                 __syncwarp();
@@ -268,11 +281,12 @@ __global__ void __launch_bounds__(kPlainWarps * 32) k_plain_train(TrainArgs a, i
                 }
                 __syncwarp();
                 merge_duplicates(negs, K, sen + lo_b, rows, grad, dup, lane);
-                // MM2: W_out[neg_k] = M_out[k] + sum_r grad[k][r] M_in[r]  (each distinct word once)
+                // MM2: W_out[neg_k] += sum_r grad[k][r] M_in[r]  (each distinct word once, added to
+                // the row as it is now, not to the staged copy)
                 for (int k = 0; k < K; k++) {
                     if (dup[k] >= 0) continue;
                     RowReg<NV2> acc;
-                    load_row(acc, m_out + (size_t) k * ld, n2, lane);
+                    load_row_g(acc, w_out + (size_t) negs[k] * ld, n2, lane);
                     for (int r = 0; r < rows; r++) {
                         RowReg<NV2> in;
                         load_row(in, m_in + (size_t) r * ld, n2, lane);
@@ -283,11 +297,11 @@ __global__ void __launch_bounds__(kPlainWarps * 32) k_plain_train(TrainArgs a, i
                     }
                     store_row(acc, w_out + (size_t) negs[k] * ld, n2, lane);
                 }
-                // MM3: W_in[sen[lo_b + r]] = M_in[r] + sum_k grad[k][r] M_out[k]
+                // MM3: W_in[sen[lo_b + r]] += sum_k grad[k][r] M_out[k]
                 for (int r = 0; r < rows; r++) {
                     if (dup[K + r] >= 0) continue;
                     RowReg<NV2> acc;
-                    load_row(acc, m_in + (size_t) r * ld, n2, lane);
+                    load_row_g(acc, w_in + (size_t) sen[lo_b + r] * ld, n2, lane);
                     for (int k = 0; k < K; k++) {
                         RowReg<NV2> o;
                         load_row(o, m_out + (size_t) k * ld, n2, lane);
