@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--no-compare", action="store_true", help="skip the plain FP32 comparison and recall")
     ap.add_argument("--cpu-sample", type=int, default=6_000_000, help="tokens in the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--min-rounds", type=int, default=0,
+                    help="parw2v_config.min_rounds (0: the library's cap on sentences in flight; -1: no cap, "
+                         "as the 800M-token corpus runs uncapped under the default)")
     return ap.parse_args()
 
 
@@ -266,6 +269,7 @@ def main():
     stream_d, counts, words, gen_ids = synth.topic_zipf_stream_torch(args.tokens, N_TYPES, N_TOPICS,
                                                                        seed=4, min_count=MIN_COUNT, device=dev)
     n = int(stream_d.numel())
+    n_sent = int(counts[0])  # one "</s>" per sentence
     stream_h = torch.empty(n, dtype=torch.int32, pin_memory=True)
     stream_h.copy_(stream_d)
     del stream_d
@@ -277,7 +281,7 @@ def main():
     d = HYPER["size"]
 
     def make(m, seed):
-        t = pw.Trainer(mode=m, device=local, seed=seed, **HYPER)
+        t = pw.Trainer(mode=m, device=local, seed=seed, min_rounds=args.min_rounds, **HYPER)
         t.set_vocab(counts)
         t.init_weights()
         t.set_corpus(stream_np)
@@ -327,9 +331,11 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "bf16" if bytes_per == 2 else "f32",
             "data": "synthetic (seeded topic-mixture Zipf corpus generated on the device)",
-            "config": {"workload": f"1B-word-shaped corpus: {args.tokens} tokens + {n - args.tokens} </s>, "
-                                   f"{V - 1} word types after min-count {MIN_COUNT}, 256 planted topics",
-                       "mode": args.mode, **HYPER, "min_count": MIN_COUNT, "corpus_tokens_with_eos": n,
+            "config": {"workload": f"1B-word-shaped corpus: {n - n_sent} tokens (of {args.tokens} generated, "
+                                   f"words under min-count {MIN_COUNT} dropped) + {n_sent} </s>, "
+                                   f"{V - 1} word types, 256 planted topics",
+                       "mode": args.mode, **HYPER, "min_count": MIN_COUNT, "min_rounds": args.min_rounds,
+                       "corpus_tokens_with_eos": n,
                        "vocab_size": V, "replicas": world,
                        "l2": "no flush: corpus (4 B/token) and weights exceed the 126 MB L2"},
             "roofline": roofline, "e2e": e2e, "gpu_launches": int(args.steps * (1 + HYPER["iter"] * 4)),
