@@ -48,6 +48,21 @@ __host__ __device__ __forceinline__ uint32_t mod_small(uint64_t x, uint32_t m) {
     return (hi * r32 % m + lo) % m;
 }
 
+// x mod d for a 64-bit x and a divisor 0 < d < 2^16 fixed for a launch, with multiplications
+// only (no integer division on the device): Lemire, Kaser & Kurz, "Faster remainder by direct
+// computation" (2019): for a 32-bit a, a mod d = high64(low64(M * a) * d), M = floor((2^64-1)/d) + 1;
+// a 64-bit x is reduced through its 32-bit halves as in mod_small.  Build it once per thread.
+struct FastMod {
+    uint64_t M;
+    uint32_t d, r32;
+    __host__ __device__ explicit FastMod(uint32_t divisor)
+        : M(~0ULL / divisor + 1), d(divisor), r32((uint32_t) (0x100000000ULL % divisor)) {}
+    __device__ __forceinline__ uint32_t mod32(uint32_t a) const { return (uint32_t) __umul64hi(M * a, d); }
+    __device__ __forceinline__ uint32_t operator()(uint64_t x) const {
+        return mod32(mod32((uint32_t) (x >> 32)) * r32 + mod32((uint32_t) x));
+    }
+};
+
 // SplitMix64 finaliser (Steele, Lea & Flood 2014): a bijective 64-bit mixer used to derive
 // independent per-token / per-sentence random streams in the Hogwild modes.
 __host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {

@@ -471,6 +471,7 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int w = a.window, B = a.batch, ld = a.ld, d = a.d;
+    const FastMod mod_w((uint32_t) w), mod_2w((uint32_t) (2 * w));
     const int n4 = (d + 3) >> 2;  // float4 chunks that carry data (the padding stays zero)
     const Layout Lo = make_layout(ld, w, a.negative, B, BF16);
     float *s_exp = reinterpret_cast<float *>(smem_raw);
@@ -624,7 +625,7 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
                     }
                 }
                 rng = lcg_next(rng);
-                const int b = (int) mod_small(rng, (uint32_t) w);
+                const int b = (int) mod_w(rng);
                 const int lo_c = max(p - w + b, 0), hi_c = min(p + w - b, L - 1);
                 const int n = hi_c - lo_c;  // contexts [lo_c, hi_c] without p, in window order
                 if constexpr (SYNC) {
@@ -735,7 +736,7 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
                 const int lo_b = nb * B;
                 const int rows = min(B, L - lo_b);
                 rng = lcg_next(rng);
-                const int rep_b = (int) mod_small(rng, (uint32_t) ((lo_b <= w - 1 || (L - 1) - lo_b <= w - 1) ? w : 2 * w));
+                const int rep_b = (int) ((lo_b <= w - 1 || (L - 1) - lo_b <= w - 1) ? mod_w(rng) : mod_2w(rng));
                 const int K = rep_b * a.negative;
                 if (!warp_draw_negatives(a.table, a.vocab, rng, sen, L, K, negs, lane, a.max_resample)) {
                     failed = true;  // unresolved negatives: leave the batch untouched
@@ -835,6 +836,7 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int w = a.window, B = a.batch, ld = a.ld, d = a.d;
+    const FastMod mod_w((uint32_t) w), mod_2w((uint32_t) (2 * w));
     const int n4 = (d + 3) >> 2;
     const Layout Lo = make_layout_stream(ld, w, a.negative, B, BF16);
     float *s_exp = reinterpret_cast<float *>(smem_raw);
@@ -869,7 +871,7 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
             // ---- attraction (:529-568) ----
             for (int p = 0; p < L; p++) {
                 rng = lcg_next(rng);
-                const int b = (int) mod_small(rng, (uint32_t) w);
+                const int b = (int) mod_w(rng);
                 const int t = __ldg(sen + p);
                 T *yrow = w_out + (size_t) t * ld;
                 Row<NV4> y;
@@ -976,7 +978,7 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                 const int lo_b = nb * B;
                 const int rows = min(B, L - lo_b);
                 rng = lcg_next(rng);
-                const int rep_b = (int) mod_small(rng, (uint32_t) ((lo_b <= w - 1 || (L - 1) - lo_b <= w - 1) ? w : 2 * w));
+                const int rep_b = (int) ((lo_b <= w - 1 || (L - 1) - lo_b <= w - 1) ? mod_w(rng) : mod_2w(rng));
                 const int K = rep_b * a.negative;
                 if (!warp_draw_negatives(a.table, a.vocab, rng, sen, L, K, negs, lane, a.max_resample)) {
                     failed = true;

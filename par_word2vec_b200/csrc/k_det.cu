@@ -73,6 +73,7 @@ __global__ void __launch_bounds__(kDetThreads, 1) k_det_train(TrainArgs a, DevTr
     __shared__ int s_ctx[256];   // and context words
     const int tid = threadIdx.x;
     const int d = a.d, ld = a.ld, w = a.window, B = a.batch;
+    const FastMod mod_w((uint32_t) w), mod_2w((uint32_t) (2 * w));  // r % w, r % 2w (:534, :591-600)
     const int kmax = 2 * w * a.negative;
     float *prod = reinterpret_cast<float *>(smem_raw);  // d
     float *grad = prod + ((d + 3) & ~3);                 // kmax * B
@@ -124,7 +125,7 @@ __global__ void __launch_bounds__(kDetThreads, 1) k_det_train(TrainArgs a, DevTr
                 }
             } else {
                 st.rng = lcg_next(st.rng);
-                st.b = (int) (st.rng % (uint64_t) w);
+                st.b = (int) mod_w(st.rng);
                 st.action = kActAttract;
                 trace_put_u8(tr.b, tr.b_cap, &a.cnt->n_b, (uint8_t) st.b);
                 unsigned long long i = a.cnt->n_alpha;
@@ -221,8 +222,8 @@ __global__ void __launch_bounds__(kDetThreads, 1) k_det_train(TrainArgs a, DevTr
                 const int rows = hi - lo + 1;
                 if (tid == 0) {
                     st.rng = lcg_next(st.rng);
-                    if (lo <= w - 1 || (len - 1) - lo <= w - 1) st.rep_b = (int) (st.rng % (uint64_t) w);
-                    else st.rep_b = (int) (st.rng % (uint64_t) (w * 2));
+                    if (lo <= w - 1 || (len - 1) - lo <= w - 1) st.rep_b = (int) mod_w(st.rng);
+                    else st.rep_b = (int) mod_2w(st.rng);
                     st.k = st.rep_b * a.negative;
                     trace_put_u8(tr.rep_b, tr.rep_b_cap, &a.cnt->n_rep_b, (uint8_t) st.rep_b);
                     a.cnt->batches++;

@@ -130,6 +130,7 @@ __global__ void __launch_bounds__(kPlainWarps * 32) k_plain_train(TrainArgs a, i
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int w = a.window, B = a.batch, ld = a.ld;
+    const FastMod mod_w((uint32_t) w), mod_2w((uint32_t) (2 * w));
     const int n2 = (a.d + 1) >> 1;
     const int kmax = 2 * w * a.negative;
     float *s_exp = reinterpret_cast<float *>(smem_raw);  // 1004
@@ -169,7 +170,7 @@ __global__ void __launch_bounds__(kPlainWarps * 32) k_plain_train(TrainArgs a, i
             // ---- attraction (:529-568) ----
             for (int pos = 0; pos < L; pos++) {
                 rng = lcg_next(rng);
-                const int b = (int) mod_small(rng, (uint32_t) w);
+                const int b = (int) mod_w(rng);
                 float *y = w_out + (size_t) sen[pos] * ld;
                 RowReg<NV2> yr;
                 load_row_g(yr, y, n2, lane);
@@ -247,7 +248,7 @@ __global__ void __launch_bounds__(kPlainWarps * 32) k_plain_train(TrainArgs a, i
                 const int lo_b = nb * B;
                 const int rows = min(B, L - lo_b);
                 rng = lcg_next(rng);
-                const int rep_b = (int) mod_small(rng, (uint32_t) ((lo_b <= w - 1 || (L - 1) - lo_b <= w - 1) ? w : 2 * w));
+                const int rep_b = (int) ((lo_b <= w - 1 || (L - 1) - lo_b <= w - 1) ? mod_w(rng) : mod_2w(rng));
                 const int K = rep_b * a.negative;
                 if (!warp_draw_negatives(a.table, a.vocab, rng, sen, L, K, negs, lane, a.max_resample)) {
                     failed = true;  // unresolved negatives: leave the batch untouched
