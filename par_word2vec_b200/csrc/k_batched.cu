@@ -137,6 +137,13 @@ struct Store<false> {  // FP32 tables
     // a row of the global tables: read at L2, never from this SM's (non-coherent) L1
     __device__ static float4 load4g(const float *row, int j4) { return __ldcg(reinterpret_cast<const float4 *>(row) + j4); }
     __device__ static void store4(float *row, int j4, float4 v, uint64_t) { reinterpret_cast<float4 *>(row)[j4] = v; }
+    // 16-byte lane chunks as stored (read ahead and kept in this form until used)
+    using Raw = float4;
+    __device__ static Raw zero_raw() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+    __device__ static Raw loadraw_g(const float *row, int j4) { return __ldcg(reinterpret_cast<const float4 *>(row) + j4); }
+    __device__ static float4 widen(Raw r) { return r; }
+    __device__ static Raw pack4(float4 v, uint64_t) { return v; }
+    __device__ static void storeraw(float *row, int j4, Raw r) { reinterpret_cast<float4 *>(row)[j4] = r; }
 };
 
 template <>
@@ -160,11 +167,19 @@ struct Store<true> {  // BF16 tables
         return widen(__ldcg(reinterpret_cast<const uint2 *>(row) + j4));
     }
     __device__ static void store4(__nv_bfloat16 *row, int j4, float4 v, uint64_t h) {
+        reinterpret_cast<uint2 *>(row)[j4] = pack4(v, h);
+    }
+    // 4 BF16 as stored (read ahead and kept in this form until used: 2 registers, not 4)
+    using Raw = uint2;
+    __device__ static Raw zero_raw() { return make_uint2(0u, 0u); }
+    __device__ static Raw loadraw_g(const __nv_bfloat16 *row, int j4) { return __ldcg(reinterpret_cast<const uint2 *>(row) + j4); }
+    __device__ static Raw pack4(float4 v, uint64_t h) {
         uint2 u;
         u.x = pack_sr2(make_float2(v.x, v.y), h);
         u.y = pack_sr2(make_float2(v.z, v.w), h >> 32);
-        reinterpret_cast<uint2 *>(row)[j4] = u;
+        return u;
     }
+    __device__ static void storeraw(__nv_bfloat16 *row, int j4, Raw r) { reinterpret_cast<uint2 *>(row)[j4] = r; }
 };
 
 
@@ -869,6 +884,16 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
             LaneBits rb{(uint32_t) mix64(rng ^ (0xA24BAED4963EE407ULL * (uint64_t) (lane + 1))) | 1u};
             const float alpha = sentence_alpha_b(a, c0, total_kept);
             // ---- attraction (:529-568) ----
+            // Rows are read one step ahead (the next target's row during this position, the next
+            // context's row during this pair), so the L2 latency overlaps the dependent chain.  A
+            // row read ahead that this warp writes before using it (the same word again) is
+            // replaced by the value written.
+            typename S::Raw yn[NV4];
+            {
+                const T *yrow0 = w_out + (size_t) __ldg(sen) * ld;
+#pragma unroll
+                for (int k = 0; k < NV4; k++) yn[k] = lane + 32 * k < n4 ? S::loadraw_g(yrow0, lane + 32 * k) : S::zero_raw();
+            }
             for (int p = 0; p < L; p++) {
                 rng = lcg_next(rng);
                 const int b = (int) mod_w(rng);
@@ -876,9 +901,12 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                 T *yrow = w_out + (size_t) t * ld;
                 Row<NV4> y;
 #pragma unroll
-                for (int k = 0; k < NV4; k++) {
-                    const int cc = lane + 32 * k;
-                    y.v[k] = cc < n4 ? S::load4g(yrow, cc) : make_float4(0.f, 0.f, 0.f, 0.f);
+                for (int k = 0; k < NV4; k++) y.v[k] = S::widen(yn[k]);
+                const int t_next = p + 1 < L ? __ldg(sen + p + 1) : t;
+                if (t_next != t) {
+                    const T *ynrow = w_out + (size_t) t_next * ld;
+#pragma unroll
+                    for (int k = 0; k < NV4; k++) yn[k] = lane + 32 * k < n4 ? S::loadraw_g(ynrow, lane + 32 * k) : S::zero_raw();
                 }
                 const int lo_c = max(p - w + b, 0), hi_c = min(p + w - b, L - 1);
                 const int n = hi_c - lo_c;
@@ -941,26 +969,48 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                     for (int k = 0; k < NV4; k++)
                         y.v[k] = make_float4(y.v[k].x + dy.v[k].x, y.v[k].y + dy.v[k].y, y.v[k].z + dy.v[k].z,
                                              y.v[k].w + dy.v[k].w);
-                } else {
+                } else if (n > 0) {
+                    // contexts c in [lo_c, hi_c] without p, in window order
+                    int c = lo_c == p ? lo_c + 1 : lo_c;
+                    int wc = __ldg(sen + c);
+                    typename S::Raw xn[NV4];
+                    {
+                        const T *xrow0 = w_in + (size_t) wc * ld;
+#pragma unroll
+                        for (int k = 0; k < NV4; k++) xn[k] = lane + 32 * k < n4 ? S::loadraw_g(xrow0, lane + 32 * k) : S::zero_raw();
+                    }
                     for (int i = 0; i < n; i++) {
-                        const int c = lo_c + i + (lo_c + i >= p ? 1 : 0);
-                        T *x = w_in + (size_t) __ldg(sen + c) * ld;
+                        const int word = wc;
+                        T *x = w_in + (size_t) word * ld;
                         Row<NV4> xr;
                         float f = 0.f;
 #pragma unroll
                         for (int k = 0; k < NV4; k++) {
-                            const int cc = lane + 32 * k;
-                            xr.v[k] = cc < n4 ? S::load4g(x, cc) : make_float4(0.f, 0.f, 0.f, 0.f);
+                            xr.v[k] = S::widen(xn[k]);
                             f = f4_dot(xr.v[k], y.v[k], f);
+                        }
+                        const bool more = i + 1 < n;
+                        if (more) {
+                            c = c + 1 == p ? c + 2 : c + 1;
+                            wc = __ldg(sen + c);
+                            if (wc != word) {
+                                const T *xnrow = w_in + (size_t) wc * ld;
+#pragma unroll
+                                for (int k = 0; k < NV4; k++)
+                                    xn[k] = lane + 32 * k < n4 ? S::loadraw_g(xnrow, lane + 32 * k) : S::zero_raw();
+                            }
                         }
                         f = warp_sum(f);
                         const float g = grad_from_table(f, 1, alpha, s_exp);
+                        const bool again = more && wc == word;
 #pragma unroll
                         for (int k = 0; k < NV4; k++) {
                             const int cc = lane + 32 * k;
                             const float4 yv = y.v[k];
                             y.v[k] = f4_fma(g, xr.v[k], yv);
-                            if (cc < n4) S::store4(x, cc, f4_fma(g, yv, xr.v[k]), rb.next());
+                            const typename S::Raw r = S::pack4(f4_fma(g, yv, xr.v[k]), rb.next());
+                            if (cc < n4) S::storeraw(x, cc, r);
+                            if (again) xn[k] = r;
                         }
                     }
                 }
@@ -968,7 +1018,9 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
 #pragma unroll
                 for (int k = 0; k < NV4; k++) {
                     const int cc = lane + 32 * k;
-                    if (cc < n4) S::store4(yrow, cc, y.v[k], rb.next());
+                    const typename S::Raw r = S::pack4(y.v[k], rb.next());
+                    if (cc < n4) S::storeraw(yrow, cc, r);
+                    if (t_next == t) yn[k] = r;
                 }
             }
             __syncwarp();  // this sentence's row writes before any lane's staging reads

@@ -1,9 +1,10 @@
 """Hogwild modes against the reference CPU Hogwild run on the same corpus.
 
-Bar (statistical, since Hogwild runs are not reproducible even on the reference):
+Bar (statistical, since Hogwild runs are not reproducible even on the reference; the reference is
+run three times and its mean is the bar):
   final SGNS loss on a fixed evaluation set within 1% of the reference's, and planted-topic
   recall@10 within 0.01 of the reference's.
-The reference is oracle/_ref/par_w2v_ref_fast (the reference source, all host threads)."""
+The reference is oracle/_ref/par_w2v_ref_fast (the reference source) at 16 threads, a fixed count: its own loss moves with the thread count."""
 import os
 import shutil
 import subprocess
@@ -18,6 +19,7 @@ from oracle import pwo
 
 pytestmark = pytest.mark.gpu
 
+REF_RUNS = 3
 FLAGS = dict(size=100, window=5, negative=5, sample="1e-4", iter=1, min_count=5, batch_size=24, alpha="0.025")
 N_TOPICS = 64
 
@@ -30,15 +32,17 @@ def text_run():
     toks, lens = synth.topic_zipf(3000, 12000, N_TOPICS, doc_len=1000, seed=21)
     corpus = os.path.join(tmp, "c.txt")
     synth.write_text(corpus, toks, lens)
-    threads = str(max(1, min(os.cpu_count() or 1, 32)))
-    args = [pwo.REF_FAST_BIN, "-train", corpus, "-output", os.path.join(tmp, "o.txt"), "-debug", "0",
-            "-threads", threads, "-binary", "1", "-dump", os.path.join(tmp, "r")]
-    for k, v in FLAGS.items():
-        args += ["-" + k.replace("_", "-"), str(v)]
-    subprocess.run(args, check=True, cwd=tmp, stdout=subprocess.DEVNULL)
-    V, d, tw, _ = map(int, open(os.path.join(tmp, "r.meta")).read().split())
-    ref_in = np.fromfile(os.path.join(tmp, "r.win"), np.float32).reshape(V, d)
-    ref_out = np.fromfile(os.path.join(tmp, "r.wout"), np.float32).reshape(V, d)
+    threads = "16"  # the reference's Hogwild loss depends on its thread count: fixed, not the box's cores
+    refs = []
+    for run in range(REF_RUNS):  # the reference's Hogwild loss varies run to run: its mean is the bar
+        args = [pwo.REF_FAST_BIN, "-train", corpus, "-output", os.path.join(tmp, "o.txt"), "-debug", "0",
+                "-threads", threads, "-binary", "1", "-dump", os.path.join(tmp, "r")]
+        for k, v in FLAGS.items():
+            args += ["-" + k.replace("_", "-"), str(v)]
+        subprocess.run(args, check=True, cwd=tmp, stdout=subprocess.DEVNULL)
+        V, d, _, _ = map(int, open(os.path.join(tmp, "r.meta")).read().split())
+        refs.append((np.fromfile(os.path.join(tmp, "r.win"), np.float32).reshape(V, d),
+                     np.fromfile(os.path.join(tmp, "r.wout"), np.float32).reshape(V, d)))
     vocab = pw.Vocab.learn(corpus, FLAGS["min_count"])
     stream = vocab.load_stream(corpus)
     words = vocab.words()
@@ -46,8 +50,11 @@ def text_run():
     labels = evaluate.labels_from_words(words, N_TOPICS)
     queries = evaluate.top_queries(counts, labels, 3000)
     triples = evaluate.eval_triples(stream, counts, n_windows=4096)
-    yield dict(tmp=tmp, V=V, d=d, ref_in=ref_in, ref_out=ref_out, stream=stream, counts=counts, labels=labels,
-               queries=queries, triples=triples)
+    run = dict(tmp=tmp, V=V, d=d, stream=stream, counts=counts, labels=labels, queries=queries, triples=triples)
+    scores = np.array([score(run, ri, ro) for ri, ro in refs])
+    run.update(ref_loss=float(scores[:, 0].mean()), ref_recall=float(scores[:, 1].mean()),
+               ref_losses=scores[:, 0].tolist())
+    yield run
     shutil.rmtree(tmp)
 
 
@@ -77,14 +84,14 @@ def train_mode(run, mode, seed=1, variant=0):
                                           (pw.MODE_BATCHED_BF16, pw.VARIANT_WINDOW),
                                           (pw.MODE_BATCHED_BF16, pw.VARIANT_STREAM)])
 def test_hogwild_matches_reference_loss_and_recall(text_run, mode, variant):
-    ref_loss, ref_rec = score(text_run, text_run["ref_in"], text_run["ref_out"])
+    ref_loss, ref_rec = text_run["ref_loss"], text_run["ref_recall"]
     st, w_in, w_out = train_mode(text_run, mode, variant=variant)
     assert np.isfinite(w_in).all() and np.isfinite(w_out).all()
     assert st["words"] == len(text_run["stream"])
     loss, rec = score(text_run, w_in, w_out)
     init_in, init_out = pwo.init_net(text_run["V"], text_run["d"])
     init_loss, _ = score(text_run, init_in, init_out)
-    print(f"mode {mode} variant {variant}: loss {loss:.5f} (ref {ref_loss:.5f}, init {init_loss:.5f}) recall {rec:.4f} (ref {ref_rec:.4f}) "
+    print(f"mode {mode} variant {variant}: loss {loss:.5f} (ref mean {ref_loss:.5f} of {text_run['ref_losses']}, init {init_loss:.5f}) recall {rec:.4f} (ref {ref_rec:.4f}) "
           f"kept {st['kept']} ms {st['kernel_ms']:.1f}")
     assert ref_loss < init_loss  # the evaluation set measures training
     assert abs(loss - ref_loss) <= 0.01 * ref_loss
