@@ -583,25 +583,58 @@ static int train_hogwild(parw2v_ctx *c, TrainArgs &a, parw2v_stats *st) {
     }
     c->last_grid = grid;
     c->last_warps = warps;
+    // One epoch is two CUDA graphs, captured once and replayed for every epoch: (reset the work
+    // counter, subsample and pack) and (train, advance the epoch index in device memory).  The
+    // timing events are recorded between the two launches, outside the graphs.
+    CK(c, cudaMemsetAsync(&c->d_cnt->epoch, 0, sizeof(unsigned), c->stream), "counters");
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    cudaError_t e = cudaSuccess;
+    for (int part = 0; part < 2 && e == cudaSuccess; part++) {
+        cudaGraph_t graph = nullptr;
+        e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) break;
+        if (part == 0) {
+            e = cudaMemsetAsync(&c->d_cnt->work, 0, sizeof(unsigned long long), c->stream);
+            if (e == cudaSuccess)
+                e = launch_pack(a, c->d_packed, c->d_line_end, c->d_tile_kept, c->d_tile_zero, pack_tiles(c->n_tokens),
+                                c->stream);
+        } else {
+            e = plain ? launch_plain_train(a, grid, warps, c->stream)
+                      : launch_batched_train(a, c->bf16, stream_variant(c), grid, warps, c->stream);
+            if (e == cudaSuccess) e = launch_advance_epoch(c->d_cnt, c->stream);
+        }
+        const cudaError_t ec = cudaStreamEndCapture(c->stream, &graph);
+        if (e == cudaSuccess) e = ec;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&exec[part], graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+    }
+    auto release = [&]() {
+        for (auto &x : exec)
+            if (x) cudaGraphExecDestroy(x);
+    };
+    if (e != cudaSuccess) {
+        release();
+        return cuda_fail(c, e, "capturing the epoch graphs");
+    }
     float pack_ms_total = 0.f, kernel_ms_total = 0.f;
     for (int ep = 0; ep < c->cfg.iter; ep++) {
-        a.epoch = ep;
-        CK(c, cudaMemsetAsync(&c->d_cnt->work, 0, sizeof(unsigned long long), c->stream), "counters");
-        CK(c, cudaEventRecord(c->ev0, c->stream), "event");
-        CK(c, launch_pack(a, c->d_packed, c->d_line_end, c->d_tile_kept, c->d_tile_zero, pack_tiles(c->n_tokens), c->stream),
-           "packing kernels");
-        CK(c, cudaEventRecord(c->ev1, c->stream), "event");
-        cudaError_t e = plain ? launch_plain_train(a, grid, warps, c->stream)
-                              : launch_batched_train(a, c->bf16, stream_variant(c), grid, warps, c->stream);
-        if (e != cudaSuccess) return cuda_fail(c, e, "training kernel launch");
-        CK(c, cudaEventRecord(c->ev2, c->stream), "event");
-        CK(c, cudaStreamSynchronize(c->stream), "training kernel");
+        e = cudaEventRecord(c->ev0, c->stream);
+        if (e == cudaSuccess) e = cudaGraphLaunch(exec[0], c->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(c->ev1, c->stream);
+        if (e == cudaSuccess) e = cudaGraphLaunch(exec[1], c->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(c->ev2, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) {
+            release();
+            return cuda_fail(c, e, "training epoch");
+        }
         float m0 = 0, m1 = 0;
         cudaEventElapsedTime(&m0, c->ev0, c->ev1);
         cudaEventElapsedTime(&m1, c->ev1, c->ev2);
         pack_ms_total += m0;
         kernel_ms_total += m1;
     }
+    release();
     DevCounters h;
     if ((rc = read_counters(c, &h))) return rc;
     if (st) {

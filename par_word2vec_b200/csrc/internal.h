@@ -22,6 +22,7 @@ struct DevCounters {
     unsigned long long total_kept;  // kept tokens after subsampling (set by packing)
     float final_alpha;
     unsigned error;                 // kErr* bits
+    unsigned epoch;                 // Hogwild modes: the epoch being trained (advanced on the device)
 };
 
 // Trace buffers on the device (DET mode)
@@ -46,7 +47,6 @@ struct TrainArgs {
     float alpha0, sample;
     uint64_t train_words;
     uint64_t seed;
-    int epoch;
     DevCounters *cnt;
     // Hogwild packing products
     const int32_t *packed;   // kept tokens in corpus order
@@ -65,6 +65,7 @@ cudaError_t launch_build_table(const double *pow_cn, int V, int32_t *table, floa
 cudaError_t launch_init_net(float *w_in, float *w_out, __nv_bfloat16 *b_in, __nv_bfloat16 *b_out, int V,
                             int d, int ld, cudaStream_t s);
 cudaError_t launch_det_train(const TrainArgs &a, const DevTrace &tr, cudaStream_t s, size_t *smem_needed);
+cudaError_t launch_advance_epoch(DevCounters *cnt, cudaStream_t s);
 cudaError_t launch_count_zeros(const int32_t *corpus, uint64_t n, DevCounters *cnt, cudaStream_t s);
 cudaError_t launch_pack(const TrainArgs &a, int32_t *packed, uint32_t *line_end, uint32_t *tile_kept,
                         uint32_t *tile_zero, uint64_t n_tiles, cudaStream_t s);

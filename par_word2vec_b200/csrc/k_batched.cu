@@ -510,6 +510,7 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
     T *w_in = static_cast<T *>(a.w_in);
     T *w_out = static_cast<T *>(a.w_out);
     const uint64_t n_lines = a.cnt->n_lines, total_kept = a.cnt->total_kept;
+    const int epoch = hogwild_epoch(a);
     const int row_chunks = ld / S::kChunkElems;  // 16-byte pieces per stored row
     const bool use_mma = Lo.mma;
     // c mod ws for positions c < 2^16 by a multiply-high reciprocal (exact: ws <= 256)
@@ -528,9 +529,9 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
         for (uint32_t c0 = lo_line; c0 < hi_line; c0 += kMaxSentence, piece++) {
             const int L = (int) min((uint32_t) kMaxSentence, hi_line - c0);
             const int32_t *sen = a.packed + c0;
-            uint64_t rng = sentence_seed_b(a, line, piece);
+            uint64_t rng = sentence_seed_b(a, epoch, line, piece);
             LaneBits rb{(uint32_t) mix64(rng ^ (0xA24BAED4963EE407ULL * (uint64_t) (lane + 1))) | 1u};
-            const float alpha = sentence_alpha_b(a, c0, total_kept);
+            const float alpha = sentence_alpha_b(a, epoch, c0, total_kept);
 
             // ---- attraction (:529-568) ----
             // One loop from p = -max(w, P) to L + w: positions join the window at step q - w (the
@@ -867,6 +868,7 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
     T *w_in = static_cast<T *>(a.w_in);
     T *w_out = static_cast<T *>(a.w_out);
     const uint64_t n_lines = a.cnt->n_lines, total_kept = a.cnt->total_kept;
+    const int epoch = hogwild_epoch(a);
     unsigned long long st_kept = 0, st_sent = 0, st_pairs = 0, st_batches = 0, st_negs = 0;
     bool failed = false;
 
@@ -880,9 +882,9 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
         for (uint32_t c0 = lo_line; c0 < hi_line; c0 += kMaxSentence, piece++) {
             const int L = (int) min((uint32_t) kMaxSentence, hi_line - c0);
             const int32_t *sen = a.packed + c0;
-            uint64_t rng = sentence_seed_b(a, line, piece);
+            uint64_t rng = sentence_seed_b(a, epoch, line, piece);
             LaneBits rb{(uint32_t) mix64(rng ^ (0xA24BAED4963EE407ULL * (uint64_t) (lane + 1))) | 1u};
-            const float alpha = sentence_alpha_b(a, c0, total_kept);
+            const float alpha = sentence_alpha_b(a, epoch, c0, total_kept);
             // ---- attraction (:529-568) ----
             // Rows are read one step ahead (the next target's row during this position, the next
             // context's row during this pair), so the L2 latency overlaps the dependent chain.  A

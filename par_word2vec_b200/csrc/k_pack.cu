@@ -31,7 +31,7 @@ __device__ __forceinline__ uint64_t keep_key(uint64_t seed, int epoch) {
 // Loads the thread's 16 tokens (zero past the end) and returns bit masks of kept / "</s>" tokens.
 __device__ __forceinline__ void token_flags(const TrainArgs &a, uint64_t base, int tok[kPerThread],
                                             unsigned &kept_mask, unsigned &zero_mask) {
-    const uint64_t key = keep_key(a.seed, a.epoch);
+    const uint64_t key = keep_key(a.seed, (int) __ldg(&a.cnt->epoch));
     kept_mask = 0;
     zero_mask = 0;
     if (base + kPerThread <= a.n_tokens) {
@@ -167,6 +167,13 @@ __global__ void k_count_zeros(const int32_t *corpus, uint64_t n, DevCounters *cn
 }  // namespace
 
 uint64_t pack_tiles(uint64_t n_tokens) { return (n_tokens + kTile - 1) / kTile; }
+
+static __global__ void k_advance_epoch(DevCounters *cnt) { cnt->epoch += 1; }
+
+cudaError_t launch_advance_epoch(DevCounters *cnt, cudaStream_t s) {
+    k_advance_epoch<<<1, 1, 0, s>>>(cnt);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_count_zeros(const int32_t *corpus, uint64_t n, DevCounters *cnt, cudaStream_t s) {
     k_count_zeros<<<148 * 4, 256, 0, s>>>(corpus, n, cnt);

@@ -20,6 +20,7 @@
 // words processed so far, :443).
 #include "common.cuh"
 #include "internal.h"
+#include "sentence.cuh"
 
 namespace parw2v {
 
@@ -69,18 +70,6 @@ __device__ __forceinline__ float dot_row(const RowReg<NV2> &a, const RowReg<NV2>
     return warp_sum(s);
 }
 
-__device__ __forceinline__ float sentence_alpha(const TrainArgs &a, uint64_t kept_before, uint64_t total_kept) {
-    // words processed so far, as the fraction of this epoch's kept tokens before the sentence
-    const double done = (double) a.epoch * (double) a.n_tokens +
-                        (total_kept ? (double) kept_before / (double) total_kept : 0.0) * (double) a.n_tokens;
-    float alpha = a.alpha0 * (float) (1.0 - done / ((double) a.iter * (double) a.train_words + 1.0));
-    const float floor_a = a.alpha0 * 0.0001f;
-    return alpha < floor_a ? floor_a : alpha;
-}
-
-__device__ __forceinline__ uint64_t sentence_seed(const TrainArgs &a, uint64_t line, int piece) {
-    return mix64(mix64(a.seed ^ (0xD1B54A32D192ED03ULL * (uint64_t) (a.epoch + 1))) ^ (line * 1024ULL + piece));
-}
 
 __host__ __device__ __forceinline__ size_t plain_warp_smem(int kmax, int B, int w) {
     return sizeof(int) * (size_t) (kMaxSentence + 2 * kmax + B) + sizeof(float) * (size_t) kmax * B +
@@ -150,6 +139,7 @@ __global__ void __launch_bounds__(kPlainWarps * 32) k_plain_train(TrainArgs a, i
     float *m_in = a.scratch + gwarp * a.scratch_per_warp;  // B x ld
     float *m_out = m_in + (size_t) B * ld;                  // kmax x ld
     const uint64_t n_lines = a.cnt->n_lines, total_kept = a.cnt->total_kept;
+    const int epoch = hogwild_epoch(a);
     unsigned long long st_kept = 0, st_sent = 0, st_pairs = 0, st_batches = 0, st_negs = 0;
     bool failed = false;
 
@@ -164,8 +154,8 @@ __global__ void __launch_bounds__(kPlainWarps * 32) k_plain_train(TrainArgs a, i
             const int L = (int) min((uint32_t) kMaxSentence, hi - c0);
             for (int i = lane; i < L; i += 32) sen[i] = a.packed[c0 + i];
             __syncwarp();
-            uint64_t rng = sentence_seed(a, line, piece);
-            const float alpha = sentence_alpha(a, c0, total_kept);
+            uint64_t rng = sentence_seed_b(a, epoch, line, piece);
+            const float alpha = sentence_alpha_b(a, epoch, c0, total_kept);
 
             // ---- attraction (:529-568) ----
             for (int pos = 0; pos < L; pos++) {
