@@ -162,12 +162,11 @@ class Vocab:
             raise ParW2VError(rc, f"cannot write {path}")
 
     def load_stream(self, train_file: str) -> np.ndarray:
+        # loadStream keeps at most train_words ids, so one pass into a buffer of that size suffices
         n = ctypes.c_uint64()
-        rc = self._lib.parw2v_load_stream(self._h, train_file.encode(), None, 0, ctypes.byref(n))
-        if rc:
-            raise ParW2VError(rc, f"cannot read {train_file}")
-        out = np.zeros(n.value, dtype=np.int32)
-        rc = self._lib.parw2v_load_stream(self._h, train_file.encode(), _ptr(out), n.value, ctypes.byref(n))
+        cap = max(1, self.train_words)
+        out = np.zeros(cap, dtype=np.int32)
+        rc = self._lib.parw2v_load_stream(self._h, train_file.encode(), _ptr(out), cap, ctypes.byref(n))
         if rc:
             raise ParW2VError(rc, f"cannot read {train_file}")
         return out[: n.value]

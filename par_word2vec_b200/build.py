@@ -81,7 +81,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         for out in ex.map(lambda c: _run(c, verbose), jobs):
             logs.append(out)
     if force or _stale(LIB, objs):
-        _run([nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"], verbose)
+        _run([nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lpthread"], verbose)
     cli_src = os.path.join(CSRC, "cli.cpp")
     if os.path.exists(cli_src) and (force or _stale(CLI, [cli_src, LIB] + hdrs)):
         _run([_cxx(), "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), cli_src, "-o", CLI,

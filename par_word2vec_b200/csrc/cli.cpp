@@ -115,10 +115,12 @@ int main(int argc, char **argv) {
         parw2v_vocab_free(vocab);
         return 0;
     }
+    // loadStream keeps at most train_words ids (PAR_Word2Vec_cpu.cpp:361): one pass into that much
     uint64_t n = 0;
-    if ((rc = parw2v_load_stream(vocab, train_file.c_str(), nullptr, 0, &n))) return die(rc, "loading the corpus", nullptr);
-    std::vector<int32_t> tokens(n ? n : 1);
-    if ((rc = parw2v_load_stream(vocab, train_file.c_str(), tokens.data(), n, &n))) return die(rc, "loading the corpus", nullptr);
+    const uint64_t cap = parw2v_vocab_train_words(vocab);
+    std::vector<int32_t> tokens(cap ? cap : 1);
+    if ((rc = parw2v_load_stream(vocab, train_file.c_str(), tokens.data(), tokens.size(), &n)))
+        return die(rc, "loading the corpus", nullptr);
     std::vector<uint32_t> counts((size_t) V);
     parw2v_vocab_counts(vocab, counts.data());
 

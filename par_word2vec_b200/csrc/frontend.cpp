@@ -1,4 +1,9 @@
-// Host front end: the reference's text handling, restated with buffered I/O.
+// Host front end: the reference's text handling, restated with buffered I/O and run on all host
+// threads.  A file is cut after newline bytes into one range per thread: a word cannot span a
+// newline, so every range tokenizes on its own exactly as the sequential reader would.  Results are
+// byte-identical to the one-thread restatement (and to the reference): vocabulary entries are
+// merged in first-occurrence order, which is the order qsort then sees; a vocabulary that would
+// reach ReduceVocab's 21M entries is learned by the sequential path instead.
 //
 //   ReadWord            PAR_Word2Vec_cpu.cpp:120-144   tokenizer ("</s>" per newline, 98-byte words)
 //   LearnVocab...       :253-292                        first-seen order, counts, ReduceVocab at 21M
@@ -11,7 +16,12 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
+#include <fcntl.h>
 #include <string>
+#include <sys/stat.h>
+#include <thread>
+#include <unistd.h>
 #include <unordered_map>
 #include <vector>
 
@@ -90,6 +100,143 @@ int vocab_compare(const void *a, const void *b) {  // VocabCompare, :199-201
     return (int) (((const VocabWord *) b)->cn - ((const VocabWord *) a)->cn);
 }
 
+// ---- parallel tokenizing ----
+
+constexpr uint64_t kMinRange = 1024;  // bytes: smaller files still take more than one range
+
+int host_threads() {
+    const unsigned n = std::thread::hardware_concurrency();
+    return (int) std::min(32u, std::max(1u, n));
+}
+
+// [begin, end) byte ranges that start after a newline byte (the first at 0), in file order.
+std::vector<std::pair<uint64_t, uint64_t>> split_at_newlines(int fd, uint64_t size, int parts) {
+    std::vector<uint64_t> cuts{0};
+    const uint64_t step = std::max<uint64_t>(kMinRange, (size + parts - 1) / std::max(1, parts));
+    std::vector<char> buf(1 << 16);
+    for (uint64_t want = step; want < size; want += step) {
+        uint64_t pos = std::max(want, cuts.back());
+        uint64_t cut = size;
+        while (pos < size) {  // the first newline at or after pos: the range ends just after it
+            const ssize_t got = pread(fd, buf.data(), std::min<uint64_t>(buf.size(), size - pos), (off_t) pos);
+            if (got <= 0) break;
+            const void *nl = memchr(buf.data(), '\n', (size_t) got);
+            if (nl) {
+                cut = pos + (uint64_t) ((const char *) nl - buf.data()) + 1;
+                break;
+            }
+            pos += (uint64_t) got;
+        }
+        if (cut >= size) break;
+        if (cut > cuts.back()) cuts.push_back(cut);
+    }
+    std::vector<std::pair<uint64_t, uint64_t>> ranges;
+    for (size_t i = 0; i < cuts.size(); i++) ranges.emplace_back(cuts[i], i + 1 < cuts.size() ? cuts[i + 1] : size);
+    return ranges;
+}
+
+// ReadWord over a byte range, calling emit(word, length) for every word and "</s>".  A range that
+// is not the file's last ends after a newline, so no word is pending at its end; at the end of the
+// file a pending word is dropped, as the reference's feof test drops it.
+template <class Emit>
+bool tokenize_range(int fd, uint64_t begin, uint64_t end, Emit &&emit) {
+    std::vector<char> buf(1 << 22);
+    char w[kMaxString];
+    int a = 0;
+    for (uint64_t pos = begin; pos < end;) {
+        const ssize_t got = pread(fd, buf.data(), std::min<uint64_t>(buf.size(), end - pos), (off_t) pos);
+        if (got <= 0) return false;
+        for (ssize_t i = 0; i < got; i++) {
+            const char ch = buf[(size_t) i];
+            if (ch == 13) continue;
+            if (ch == ' ' || ch == '\t' || ch == '\n') {
+                if (a > 0) {
+                    emit(w, strnlen(w, (size_t) a));
+                    a = 0;
+                }
+                if (ch == '\n') emit("</s>", 4);
+                continue;
+            }
+            w[a] = ch;
+            a++;
+            if (a >= kMaxString - 1) a--;
+        }
+        pos += (uint64_t) got;
+    }
+    return true;
+}
+
+// Open-addressing word -> entry table over a byte arena; entries keep first-insertion order.
+class WordTable {
+   public:
+    struct Entry {
+        uint64_t off;
+        uint32_t len;
+        uint64_t count;
+    };
+    WordTable() { slots_.assign(1 << 12, -1); }
+    static uint64_t hash(const char *s, size_t n) {  // FNV-1a, 64 bit
+        uint64_t h = 1469598103934665603ULL;
+        for (size_t i = 0; i < n; i++) h = (h ^ (unsigned char) s[i]) * 1099511628211ULL;
+        return h;
+    }
+    // index of the word's entry, inserting it (count 0) if absent
+    int64_t find_or_add(const char *s, size_t n) {
+        if ((entries_.size() + 1) * 2 > slots_.size()) grow();
+        size_t i = (size_t) hash(s, n) & (slots_.size() - 1);
+        for (;;) {
+            const int64_t e = slots_[i];
+            if (e < 0) {
+                slots_[i] = (int64_t) entries_.size();
+                entries_.push_back(Entry{(uint64_t) arena_.size(), (uint32_t) n, 0});
+                arena_.insert(arena_.end(), s, s + n);
+                return (int64_t) entries_.size() - 1;
+            }
+            const Entry &x = entries_[(size_t) e];
+            if (x.len == n && memcmp(arena_.data() + x.off, s, n) == 0) return e;
+            i = (i + 1) & (slots_.size() - 1);
+        }
+    }
+    int64_t find(const char *s, size_t n) const {
+        size_t i = (size_t) hash(s, n) & (slots_.size() - 1);
+        for (;;) {
+            const int64_t e = slots_[i];
+            if (e < 0) return -1;
+            const Entry &x = entries_[(size_t) e];
+            if (x.len == n && memcmp(arena_.data() + x.off, s, n) == 0) return e;
+            i = (i + 1) & (slots_.size() - 1);
+        }
+    }
+    std::vector<Entry> &entries() { return entries_; }
+    const char *text(const Entry &e) const { return arena_.data() + e.off; }
+
+   private:
+    void grow() {
+        std::vector<int64_t> next(slots_.size() * 2, -1);
+        for (size_t k = 0; k < entries_.size(); k++) {
+            size_t i = (size_t) hash(arena_.data() + entries_[k].off, entries_[k].len) & (next.size() - 1);
+            while (next[i] >= 0) i = (i + 1) & (next.size() - 1);
+            next[i] = (int64_t) k;
+        }
+        slots_.swap(next);
+    }
+    std::vector<int64_t> slots_;
+    std::vector<Entry> entries_;
+    std::vector<char> arena_;
+};
+
+int open_sized(const char *path, uint64_t *size) {
+    const int fd = open(path, O_RDONLY);
+    if (fd < 0) return -1;
+    struct stat st;
+    if (fstat(fd, &st) != 0) {
+        close(fd);
+        return -1;
+    }
+    *size = (uint64_t) st.st_size;
+    return fd;
+}
+
 }  // namespace
 
 struct parw2v_vocab {
@@ -140,11 +287,8 @@ struct parw2v_vocab {
     }
 };
 
-extern "C" {
-
-int parw2v_vocab_learn(const char *train_file, int min_count, parw2v_vocab **out) {
-    if (!train_file || !out) return PARW2V_ERR_ARG;
-    *out = nullptr;
+// LearnVocabFromTrainFile one word at a time (the reference's order of events, ReduceVocab included)
+static int vocab_learn_sequential(const char *train_file, int min_count, parw2v_vocab **out) {
     FILE *f = fopen(train_file, "rb");
     if (!f) return PARW2V_ERR_IO;
     parw2v_vocab *v = new parw2v_vocab();
@@ -161,6 +305,48 @@ int parw2v_vocab_learn(const char *train_file, int min_count, parw2v_vocab **out
         if ((long long) v->words.size() > kReduceAt) v->reduce(min_reduce);
     }
     fclose(f);
+    v->sort_and_filter(min_count);
+    *out = v;
+    return PARW2V_OK;
+}
+
+extern "C" {
+
+int parw2v_vocab_learn(const char *train_file, int min_count, parw2v_vocab **out) {
+    if (!train_file || !out) return PARW2V_ERR_ARG;
+    *out = nullptr;
+    uint64_t size = 0;
+    const int fd = open_sized(train_file, &size);
+    if (fd < 0) return PARW2V_ERR_IO;
+    const auto ranges = split_at_newlines(fd, size, host_threads());
+    // count every range on its own thread, words in their first-seen order
+    std::vector<WordTable> tables(ranges.size());
+    std::vector<char> ok(ranges.size(), 1);
+    std::vector<std::thread> pool;
+    for (size_t r = 0; r < ranges.size(); r++)
+        pool.emplace_back([&, r]() {
+            WordTable &t = tables[r];
+            ok[r] = tokenize_range(fd, ranges[r].first, ranges[r].second,
+                                   [&](const char *w, size_t n) { t.entries()[(size_t) t.find_or_add(w, n)].count++; });
+        });
+    for (auto &th : pool) th.join();
+    close(fd);
+    for (char k : ok)
+        if (!k) return PARW2V_ERR_IO;
+    // merge in range order: a word's index is its first occurrence in the file; "</s>" is entry 0
+    WordTable all;
+    all.entries()[(size_t) all.find_or_add("</s>", 4)].count = 0;
+    for (auto &t : tables) {
+        for (const auto &e : t.entries()) all.entries()[(size_t) all.find_or_add(t.text(e), e.len)].count += e.count;
+        t = WordTable();
+    }
+    if ((long long) all.entries().size() > kReduceAt) return vocab_learn_sequential(train_file, min_count, out);
+    parw2v_vocab *v = new parw2v_vocab();
+    v->words.reserve(all.entries().size());
+    for (const auto &e : all.entries()) {
+        const std::string w(all.text(e), e.len);
+        v->words[(size_t) v->add(w)].cn = (unsigned) e.count;
+    }
     v->sort_and_filter(min_count);
     *out = v;
     return PARW2V_OK;
@@ -229,27 +415,41 @@ int parw2v_vocab_save(const parw2v_vocab *v, const char *path) {
 int parw2v_load_stream(const parw2v_vocab *v, const char *train_file, int32_t *tokens, uint64_t capacity,
                        uint64_t *n_tokens) {
     if (!v || !train_file || !n_tokens) return PARW2V_ERR_ARG;
-    FILE *f = fopen(train_file, "rb");
-    if (!f) return PARW2V_ERR_IO;
-    Reader r(f);
-    std::string w;
+    uint64_t size = 0;
+    const int fd = open_sized(train_file, &size);
+    if (fd < 0) return PARW2V_ERR_IO;
+    // the vocabulary as a word -> id table the threads share read-only
+    WordTable ids;
+    for (const auto &e : v->words) ids.find_or_add(e.word, strlen(e.word));
+    const auto ranges = split_at_newlines(fd, size, host_threads());
+    std::vector<std::vector<int32_t>> part(ranges.size());
+    std::vector<uint64_t> count(ranges.size(), 0);
+    std::vector<char> ok(ranges.size(), 1);
+    std::vector<std::thread> pool;
+    for (size_t r = 0; r < ranges.size(); r++)
+        pool.emplace_back([&, r]() {
+            ok[r] = tokenize_range(fd, ranges[r].first, ranges[r].second, [&](const char *w, size_t n) {
+                const int64_t id = ids.find(w, n);
+                if (id < 0) return;  // out of the vocabulary: skipped (:365)
+                if (tokens) part[r].push_back((int32_t) id);
+                count[r]++;
+            });
+        });
+    for (auto &th : pool) th.join();
+    close(fd);
+    for (char k : ok)
+        if (!k) return PARW2V_ERR_IO;
+    // loadStream keeps at most train_words ids (:361)
     uint64_t n = 0;
     const uint64_t total = v->train_words;
-    while (!r.eof() && n < total) {  // loadStream, :361
-        read_word(r, w);
-        if (r.eof()) break;
-        auto it = v->index.find(w);
-        if (it == v->index.end()) continue;
+    for (size_t r = 0; r < ranges.size() && n < total; r++) {
+        const uint64_t take = std::min<uint64_t>(count[r], total - n);
         if (tokens) {
-            if (n >= capacity) {
-                fclose(f);
-                return PARW2V_ERR_CAPACITY;
-            }
-            tokens[n] = it->second;
+            if (n + take > capacity) return PARW2V_ERR_CAPACITY;
+            memcpy(tokens + n, part[r].data(), sizeof(int32_t) * take);
         }
-        n++;
+        n += take;
     }
-    fclose(f);
     *n_tokens = n;
     return PARW2V_OK;
 }
@@ -260,18 +460,37 @@ int parw2v_save_model(const parw2v_vocab *v, const float *w_in, int size, int bi
     if (!fo) return PARW2V_ERR_IO;
     const int V = (int) v->words.size();
     fprintf(fo, "%d %d\n", V, size);
-    std::vector<char> line;
-    for (int a = 0; a < V; a++) {
-        fprintf(fo, "%s ", v->words[(size_t) a].word);
-        const float *row = w_in + (size_t) a * size;
-        if (binary) {
-            fwrite(row, sizeof(float), (size_t) size, fo);
-        } else {
-            for (int b = 0; b < size; b++) fprintf(fo, "%f ", row[b]);
-        }
-        fprintf(fo, "\n");
+    // blocks of rows are formatted by the host threads ("%s " then "%f " per value, or the raw
+    // floats) and written in row order
+    const int threads = host_threads();
+    const int block = 4096;
+    std::vector<std::string> out((size_t) threads);
+    bool io_ok = true;
+    for (int b0 = 0; b0 < V && io_ok; b0 += block * threads) {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < threads; t++)
+            pool.emplace_back([&, t]() {
+                std::string &o = out[(size_t) t];
+                o.clear();
+                char num[64];
+                const int lo = b0 + t * block, hi = std::min(V, lo + block);
+                for (int a = lo; a < hi; a++) {
+                    o += v->words[(size_t) a].word;
+                    o += ' ';
+                    const float *row = w_in + (size_t) a * size;
+                    if (binary) {
+                        o.append(reinterpret_cast<const char *>(row), sizeof(float) * (size_t) size);
+                    } else {
+                        for (int k = 0; k < size; k++) o.append(num, (size_t) snprintf(num, sizeof(num), "%f ", row[k]));
+                    }
+                    o += '\n';
+                }
+            });
+        for (auto &th : pool) th.join();
+        for (const auto &o : out)
+            if (!o.empty() && fwrite(o.data(), 1, o.size(), fo) != o.size()) io_ok = false;
     }
-    return fclose(fo) == 0 ? PARW2V_OK : PARW2V_ERR_IO;
+    return (fclose(fo) == 0 && io_ok) ? PARW2V_OK : PARW2V_ERR_IO;
 }
 
 }  // extern "C"
