@@ -62,7 +62,7 @@ typedef struct {
     size_t mem_cap_bytes; /* refuse device allocations beyond this total, 0 = no cap */
     int min_rounds;  /* Hogwild modes: cap on sentences in flight, so that a small corpus is not
                         processed almost all at once from stale weights.  0 = default:
-                        max(10,000 corpus tokens' worth of lines, lines / 8192); > 0: lines /
+                        max(7,000 corpus tokens' worth of lines, lines / 8192); > 0: lines /
                         min_rounds; < 0: no cap */
     int attraction;  /* PARW2V_ATTRACT_*: how the contexts of one target are applied */
     int variant;     /* BATCHED modes: PARW2V_VARIANT_* kernel organisation */

@@ -531,15 +531,15 @@ static bool stream_variant(const parw2v_ctx *c) { return c->cfg.variant != PARW2
 // Sentences in flight for the Hogwild modes, 0 = no cap.  Concurrency acts like extra step size on
 // frequently updated rows (every sentence in flight computes its update from values the others
 // have not yet changed), so the final loss falls below the reference's as it grows.  Measured
-// against the reference's 16-32 thread runs: ~10,000 corpus tokens in flight keeps a small
-// corpus (3M-token text, 8M-token graph walks) within 1%, and an 800M-token corpus stays within
-// 1% with every warp of the device busy.  Default: max(10,000 tokens' worth of lines,
+// against the reference's 16-thread runs: ~7,000 corpus tokens in flight centres a small corpus
+// (3M-token text, 8M-token graph walks) on the reference's loss, and an 800M-token corpus stays
+// within 1% with every warp of the device busy.  Default: max(7,000 tokens' worth of lines,
 // lines / 8192); min_rounds > 0 caps at lines / min_rounds instead; min_rounds < 0: no cap.
 static uint64_t hogwild_cap(int min_rounds, uint64_t n_lines, uint64_t n_tokens) {
     if (min_rounds < 0) return 0;
     if (min_rounds > 0) return std::max<uint64_t>(1, n_lines / (uint64_t) min_rounds);
     const uint64_t per_line = std::max<uint64_t>(1, n_tokens / std::max<uint64_t>(1, n_lines));
-    return std::max<uint64_t>(std::max<uint64_t>(1, 10000 / per_line), n_lines / 8192);
+    return std::max<uint64_t>(std::max<uint64_t>(1, 7000 / per_line), n_lines / 8192);
 }
 
 static int train_hogwild(parw2v_ctx *c, TrainArgs &a, parw2v_stats *st) {

@@ -48,9 +48,16 @@ constexpr int kMmaR = 32;        // batch rows handled by the mma path (2 m-tile
 constexpr int kMmaCols = 32;     // column chunk of the staging
 constexpr int kMmaStride = 40;   // staged row stride in bf16 (80 B: conflict-free ldmatrix rows)
 constexpr int kGbStride = 40;    // bf16 G row stride (80 B)
+__host__ __device__ constexpr size_t up16_c(size_t x) { return (x + 15) & ~(size_t) 15; }
+// FP32 tables on the tensor cores (3xTF32): the same staging bytes hold 16 FP32 columns
+constexpr int kF32Cols = 16;     // column chunk of the FP32 staging
+constexpr int kF32Stride = 20;   // staged FP32 row stride in floats (80 B: conflict-free ldmatrix rows)
+constexpr int kGps = 36;         // FP32 G row stride in floats (144 B: conflict-free ldmatrix rows)
+static_assert(kF32Stride * 4 == kMmaStride * 2, "FP32 and BF16 staging rows take the same bytes");
 
-__host__ __device__ inline bool mma_path(int kmax_eff, int batch, bool bf16) {
-    return bf16 && kmax_eff <= kMmaK && batch <= kMmaR;
+__host__ __device__ inline bool mma_path(int kmax_eff, int batch) { return kmax_eff <= kMmaK && batch <= kMmaR; }
+__host__ __device__ inline size_t mma_g_bytes(bool bf16) {  // G kept through pass 2
+    return bf16 ? up16_c((size_t) kMmaK * kGbStride * 2) : up16_c((size_t) kMmaK * kGps * 4);
 }
 
 struct Layout {  // per-warp shared-memory carve-up, in bytes (all offsets 16-byte aligned)
@@ -81,13 +88,13 @@ __host__ __device__ inline Layout make_layout(int ld, int window, int negative, 
     if (ch > ((ld + 3) / 4) * 4) ch = ((ld + 3) / 4) * 4;
     if (ch < 16) ch = 16;
     L.ch = (int) ch;
-    L.mma = mma_path((2 * window - 1) * negative, batch, bf16);
+    L.mma = mma_path((2 * window - 1) * negative, batch);
     size_t rep_bytes = up16(rows_rep * (size_t) (L.ch + 4) * 4);
     L.gb_off = 0;
     if (L.mma) {
         const size_t stage = up16((size_t) (kMmaR + kMmaK) * kMmaStride * 2);
         L.gb_off = stage;
-        rep_bytes = stage + up16((size_t) kMmaK * kGbStride * 2);
+        rep_bytes = stage + mma_g_bytes(bf16);
     }
     L.region = win_total > rep_bytes ? win_total : rep_bytes;
     L.tgt_off = L.region;
@@ -396,6 +403,186 @@ __device__ __noinline__ void repel_mma(const TrainArgs &a, const Layout &Lo, uns
                 const float v0 = (k < K && r < rows) ? Gf[k * kMmaR + r] : 0.f;
                 const float v1 = (k < K && r + 1 < rows) ? Gf[k * kMmaR + r + 1] : 0.f;
                 reinterpret_cast<__nv_bfloat162 *>(Gb)[i] = __floats2bfloat162_rn(v0, v1);
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// Repulsion of one batch on the tensor cores with FP32 tables (K <= 48 negatives, rows <= 32): the
+// structure of repel_mma with FP32 staging (16-column chunks) and 3xTF32 products, so the FP32 mode
+// keeps FP32-level arithmetic.  G stays FP32 through pass 2 (kMmaK x kGps floats), and the new
+// values (staged value + update) go from the accumulators straight to the rows.
+__device__ __noinline__ void repel_mma_f32(const TrainArgs &a, const Layout &Lo, unsigned char *base, const int32_t *bw,
+                                           int rows, const int *negs, int K, float alpha, const float *s_exp, float *Gf,
+                                           int *dup, int lane) {
+    float *w_in = static_cast<float *>(a.w_in);
+    float *w_out = static_cast<float *>(a.w_out);
+    const int ld = a.ld;
+    float *sin = reinterpret_cast<float *>(base);             // kMmaR x kF32Stride
+    float *sout = sin + (size_t) kMmaR * kF32Stride;          // kMmaK x kF32Stride
+    float *Gp = reinterpret_cast<float *>(base + Lo.gb_off);  // kMmaK x kGps
+    const int g = lane >> 2, t = lane & 3;
+    const int mt1 = (K + 15) >> 4;  // m-tiles of negatives
+    const int nt1 = (rows + 7) >> 3;  // n-tiles of batch rows (pass 1)
+    const int kr8 = (rows + 7) >> 3;  // 8-row k-steps over the batch rows
+    const int kk8 = (K + 7) >> 3;     // 8-row k-steps over the negatives
+    const int mr = (rows + 15) >> 4;  // m-tiles of batch rows (pass 2)
+    constexpr int kPieces = kF32Cols / 4;  // 16-byte pieces per staged row
+    float acc[3][4][4];
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) acc[i][j][e] = 0.f;
+    __syncwarp();
+#pragma unroll 1
+    for (int pass = 0; pass < 2; pass++) {
+        // zero the staging: padding rows stay zero for every chunk of the pass
+        for (int i = lane; i < (kMmaR + kMmaK) * kF32Stride / 4; i += 32)
+            reinterpret_cast<float4 *>(sin)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        __syncwarp();
+#pragma unroll 1
+        for (int col0 = 0; col0 < ld; col0 += kF32Cols) {
+            for (int it = lane; it < (rows + K) * kPieces; it += 32) {
+                const int rr = it / kPieces, pc = it - rr * kPieces;
+                float *dst = (rr < rows ? sin + (size_t) rr * kF32Stride : sout + (size_t) (rr - rows) * kF32Stride) + pc * 4;
+                const int col = col0 + pc * 4;
+                if (col < ld) {
+                    const float *src = (rr < rows ? w_in + (size_t) __ldg(bw + rr) * ld : w_out + (size_t) negs[rr - rows] * ld) + col;
+                    cp_async16(dst, src);
+                } else {
+                    *reinterpret_cast<float4 *>(dst) = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+            }
+            cp_async_commit();
+            cp_async_wait_all();
+            __syncwarp();
+            if (pass == 0) {
+                // S += M_out . M_in^T over these 16 columns: two k-steps of 8
+#pragma unroll 1
+                for (int ks = 0; ks < kF32Cols / 8; ks++) {
+                    unsigned bb[4][2], bs[4][2];
+#pragma unroll
+                    for (int np = 0; np < 2; np++) {  // n-tiles 2np, 2np+1 in one ldmatrix.x4
+                        float r[4];
+                        const int n = np * 16 + (lane & 7) + ((lane >> 4) << 3);
+                        ldsm_x4_f32(r, sin + (size_t) n * kF32Stride + ks * 8 + ((lane >> 3) & 1) * 4);
+#pragma unroll
+                        for (int h = 0; h < 2; h++) {
+                            split_tf32(r[2 * h], bb[2 * np + h][0], bs[2 * np + h][0]);
+                            split_tf32(r[2 * h + 1], bb[2 * np + h][1], bs[2 * np + h][1]);
+                        }
+                    }
+#pragma unroll
+                    for (int mt = 0; mt < 3; mt++)
+                        if (mt < mt1) {
+                            float af[4];
+                            ldsm_x4_f32(af, sout + (size_t) (mt * 16 + (lane & 7) + ((lane >> 3) & 1) * 8) * kF32Stride + ks * 8 +
+                                                (lane >> 4) * 4);
+                            unsigned ab[4], as[4];
+                            split_a(af, ab, as);
+#pragma unroll
+                            for (int nt = 0; nt < 4; nt++)
+                                if (nt < nt1) mma3xtf32(acc[mt][nt], ab, as, bb[nt], bs[nt]);
+                        }
+                }
+            } else {
+#pragma unroll 1
+                for (int nt = 0; nt < kF32Cols / 8; nt++) {
+                    const int cb = nt * 8;
+                    if (col0 + cb >= ld) break;
+                    float o[3][4], q[2][4];
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        o[0][e] = o[1][e] = o[2][e] = 0.f;
+                        q[0][e] = q[1][e] = 0.f;
+                    }
+                    // M_out update: G (K x rows) . M_in (rows x 8 columns)
+#pragma unroll 1
+                    for (int ks = 0; ks < kr8; ks++) {
+                        unsigned bb[2], bs[2];
+                        split_tf32(sin[(size_t) (ks * 8 + t) * kF32Stride + cb + g], bb[0], bs[0]);
+                        split_tf32(sin[(size_t) (ks * 8 + t + 4) * kF32Stride + cb + g], bb[1], bs[1]);
+#pragma unroll
+                        for (int mt = 0; mt < 3; mt++)
+                            if (mt < mt1) {
+                                float af[4];
+                                ldsm_x4_f32(af, Gp + (size_t) (mt * 16 + (lane & 7) + ((lane >> 3) & 1) * 8) * kGps + ks * 8 +
+                                                    (lane >> 4) * 4);
+                                unsigned ab[4], as[4];
+                                split_a(af, ab, as);
+                                mma3xtf32(o[mt], ab, as, bb, bs);
+                            }
+                    }
+                    // M_in update: G^T (rows x K) . M_out (K x 8 columns)
+#pragma unroll 1
+                    for (int ks = 0; ks < kk8; ks++) {
+                        unsigned bb[2], bs[2];
+                        split_tf32(sout[(size_t) (ks * 8 + t) * kF32Stride + cb + g], bb[0], bs[0]);
+                        split_tf32(sout[(size_t) (ks * 8 + t + 4) * kF32Stride + cb + g], bb[1], bs[1]);
+#pragma unroll
+                        for (int mt = 0; mt < 2; mt++)
+                            if (mt < mr) {
+                                const float *gk = Gp + (size_t) (ks * 8 + t) * kGps + mt * 16 + g;
+                                const float af[4] = {gk[0], gk[8], gk[4 * kGps], gk[4 * kGps + 8]};
+                                unsigned ab[4], as[4];
+                                split_a(af, ab, as);
+                                mma3xtf32(q[mt], ab, as, bb, bs);
+                            }
+                    }
+                    // staged value + update, straight to the rows (each distinct word once)
+                    const int c = cb + 2 * t;
+                    if (col0 + c < ld) {
+#pragma unroll
+                        for (int mt = 0; mt < 3; mt++)
+                            if (mt < mt1)
+#pragma unroll
+                                for (int h = 0; h < 2; h++) {
+                                    const int row = mt * 16 + g + 8 * h;
+                                    if (row < K && dup[row] < 0) {
+                                        const float2 old = *reinterpret_cast<const float2 *>(sout + (size_t) row * kF32Stride + c);
+                                        *reinterpret_cast<float2 *>(w_out + (size_t) negs[row] * ld + col0 + c) =
+                                            make_float2(old.x + o[mt][2 * h], old.y + o[mt][2 * h + 1]);
+                                    }
+                                }
+#pragma unroll
+                        for (int mt = 0; mt < 2; mt++)
+                            if (mt < mr)
+#pragma unroll
+                                for (int h = 0; h < 2; h++) {
+                                    const int row = mt * 16 + g + 8 * h;
+                                    if (row < rows && dup[K + row] < 0) {
+                                        const float2 old = *reinterpret_cast<const float2 *>(sin + (size_t) row * kF32Stride + c);
+                                        *reinterpret_cast<float2 *>(w_in + (size_t) __ldg(bw + row) * ld + col0 + c) =
+                                            make_float2(old.x + q[mt][2 * h], old.y + q[mt][2 * h + 1]);
+                                    }
+                                }
+                    }
+                }
+            }
+            __syncwarp();
+        }
+        if (pass == 0) {
+            // raw dot products into Gf (kMmaK x kMmaR), sigma / label 0, merge repeats, then the FP32
+            // copy that pass 2 reads (zero outside K x rows)
+#pragma unroll
+            for (int mt = 0; mt < 3; mt++)
+#pragma unroll
+                for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+                    for (int e = 0; e < 4; e++)
+                        if (mt < mt1 && nt < nt1)
+                            Gf[(mt * 16 + g + ((e >> 1) << 3)) * kMmaR + nt * 8 + 2 * t + (e & 1)] = acc[mt][nt][e];
+            __syncwarp();
+            for (int i = lane; i < K * kMmaR; i += 32)
+                if ((i & (kMmaR - 1)) < rows) Gf[i] = grad_from_table(Gf[i], 0, alpha, s_exp);
+            __syncwarp();
+            merge_repeats(negs, K, bw, rows, Gf, kMmaR, dup, lane);
+            for (int i = lane; i < kMmaK * kMmaR; i += 32) {
+                const int k = i / kMmaR, r = i - k * kMmaR;
+                Gp[(size_t) k * kGps + r] = (k < K && r < rows) ? Gf[i] : 0.f;
             }
             __syncwarp();
         }
@@ -767,7 +954,10 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
                         else
                             repel_simt<true>(a, Lo, base, sen + lo_b, rows, negs, K, alpha, s_exp, G, dup, lane, rb);
                     } else {
-                        repel_simt<false>(a, Lo, base, sen + lo_b, rows, negs, K, alpha, s_exp, G, dup, lane, rb);
+                        if (use_mma)
+                            repel_mma_f32(a, Lo, base, sen + lo_b, rows, negs, K, alpha, s_exp, G, dup, lane);
+                        else
+                            repel_simt<false>(a, Lo, base, sen + lo_b, rows, negs, K, alpha, s_exp, G, dup, lane, rb);
                     }
                 }
                 __threadfence_block();
@@ -817,7 +1007,7 @@ __host__ __device__ inline Layout make_layout_stream(int ld, int window, int neg
     Layout L;
     L.ws = 0;
     L.kmax = 2 * window * negative;
-    L.mma = mma_path((2 * window - 1) * negative, batch, bf16);
+    L.mma = mma_path((2 * window - 1) * negative, batch);
     L.raw_off = 0;
     L.tgt_off = 0;
     L.meta_off = 0;
@@ -829,7 +1019,7 @@ __host__ __device__ inline Layout make_layout_stream(int ld, int window, int neg
     L.ch = (int) ch;
     if (L.mma) {
         L.gb_off = kStreamStage;
-        L.region = kStreamStage + up16((size_t) kMmaK * kGbStride * 2);
+        L.region = kStreamStage + mma_g_bytes(bf16);
         L.g_off = 0;  // the FP32 G of pass 1 shares the staging bytes
     } else {
         L.gb_off = 0;
@@ -1047,7 +1237,10 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                         else
                             repel_simt<true>(a, Lo, base, sen + lo_b, rows, negs, K, alpha, s_exp, G, dup, lane, rb);
                     } else {
-                        repel_simt<false>(a, Lo, base, sen + lo_b, rows, negs, K, alpha, s_exp, G, dup, lane, rb);
+                        if (Lo.mma)
+                            repel_mma_f32(a, Lo, base, sen + lo_b, rows, negs, K, alpha, s_exp, G, dup, lane);
+                        else
+                            repel_simt<false>(a, Lo, base, sen + lo_b, rows, negs, K, alpha, s_exp, G, dup, lane, rb);
                     }
                 }
                 __syncwarp();

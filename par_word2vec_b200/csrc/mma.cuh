@@ -54,4 +54,45 @@ __device__ __forceinline__ void mma16816(float (&d)[4], const unsigned (&a)[4], 
                  : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
+
+// ---- FP32 operands on the tensor cores: 3xTF32 ----
+// x = big + small with both parts TF32 (cvt.rna), and a*b ~ big_a*big_b + big_a*small_b +
+// small_a*big_b: the products keep about FP32's precision (the dropped small*small term is below
+// 2^-22 of the product) at three m16n8k8 TF32 MMAs.
+__device__ __forceinline__ unsigned tf32_bits(float x) {
+    unsigned r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ void split_tf32(float x, unsigned &big, unsigned &small) {
+    big = tf32_bits(x);
+    small = tf32_bits(x - __uint_as_float(big));
+}
+// D += A (16x8 tf32, row) * B (8x8 tf32, col), FP32 accumulate
+__device__ __forceinline__ void mma1688(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
+    asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                 "{%0,%1,%2,%3};"
+                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+// split FP32 fragments for 3xTF32
+__device__ __forceinline__ void split_a(const float (&a)[4], unsigned (&big)[4], unsigned (&small)[4]) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) split_tf32(a[i], big[i], small[i]);
+}
+__device__ __forceinline__ void mma3xtf32(float (&d)[4], const unsigned (&abig)[4], const unsigned (&asmall)[4],
+                                          const unsigned (&bbig)[2], const unsigned (&bsmall)[2]) {
+    mma1688(d, asmall, bbig[0], bbig[1]);
+    mma1688(d, abig, bsmall[0], bsmall[1]);
+    mma1688(d, abig, bbig[0], bbig[1]);
+}
+// ldmatrix of 32-bit elements: an 8 x 4 block of floats is an 8 x 8 block of 16-bit halves, so a
+// lane receives the float at (its row / 4, its lane % 4) of each block
+__device__ __forceinline__ void ldsm_x4_f32(float (&r)[4], const void *p) {
+    unsigned u[4];
+    ldsm_x4(u, p);
+#pragma unroll
+    for (int i = 0; i < 4; i++) r[i] = __uint_as_float(u[i]);
+}
+
 }  // namespace parw2v
