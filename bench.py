@@ -359,6 +359,18 @@ def main():
                                   "recall_at_10": evaluate.recall_at_10(w_plain, labels, queries, device=dev),
                                   "steps": 1, "note": "first epoch from InitNet, same corpus"}
             line["speedup_vs_plain"] = value / line["plain_fp32"]["value"]
+        if mode == pw.MODE_BATCHED_BF16:
+            # the batched FP32 configuration on the same corpus (FP32 tables, same kernels otherwise)
+            tf = make(pw.MODE_BATCHED, 1)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            st = tf.train()
+            f_ms = (time.perf_counter() - t0) * 1e3
+            w_f32 = tf.get_weights("in")
+            tf.close()
+            line["batched_fp32"] = {"value": n / (f_ms / 1e3), "unit": "words/s", "kernel_ms": st["kernel_ms"],
+                                    "recall_at_10": evaluate.recall_at_10(w_f32, labels, queries, device=dev),
+                                    "steps": 1, "note": "first epoch from InitNet, same corpus"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = host_threads()
         with tempfile.TemporaryDirectory() as tmp:
