@@ -174,6 +174,17 @@ int parw2v_loss_fd(parw2v_ctx *ctx, const int32_t *tgt, const int32_t *ctxw, int
                    const int32_t *neg, int n_neg, int ctx_per_window, const int32_t *matrix,
                    const int32_t *row, const int32_t *col, int n_probes, double h, double *grad);
 
+/* ---- Random walks for the graph workload (no counterpart in the reference: it trains on walk
+ * files made by other tools, data.sh:7-11) ----
+ * walks_per_node * n_nodes uniform random walks of walk_len nodes over the graph in CSR form
+ * (indptr[n_nodes + 1] starting at 0, indices[indptr[n_nodes]] neighbour ids), computed on
+ * the GPU `device`.  Walk w starts at node w mod n_nodes; step s picks neighbour
+ * (hi32(h) * degree) >> 32 with h = mix64(seed ^ mix64(w * 2^20 + s)) (SplitMix64 finaliser), so
+ * every walk is reproducible on its own.  A node without neighbours repeats to the walk's end.
+ * out_nodes receives walks_per_node * n_nodes * walk_len ids, walk after walk (host memory). */
+int parw2v_random_walks(const int64_t *indptr, const int32_t *indices, int n_nodes, int walks_per_node,
+                        int walk_len, uint64_t seed, int device, int32_t *out_nodes);
+
 /* ---- Allocation-free deterministic training (no counterpart in the reference) ----
  * For callers that cannot let a library allocate device memory: a framework whose caching
  * allocator owns the GPU's memory, or a service that reserves its memory at start-up and must not

@@ -35,7 +35,7 @@ EXPORTED = [
     "parw2v_loss", "parw2v_loss_adjoint", "parw2v_loss_fd", "parw2v_vocab_learn", "parw2v_vocab_read",
     "parw2v_vocab_free", "parw2v_vocab_size", "parw2v_vocab_train_words", "parw2v_vocab_counts",
     "parw2v_vocab_word", "parw2v_vocab_save", "parw2v_load_stream", "parw2v_save_model",
-    "parw2v_det_train_noalloc",
+    "parw2v_det_train_noalloc", "parw2v_random_walks",
 ]
 
 
@@ -98,6 +98,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "parw2v_load_stream": ([P, ctypes.c_char_p, P, U64, P], I),
         "parw2v_save_model": ([P, P, I, I, ctypes.c_char_p], I),
         "parw2v_det_train_noalloc": ([P, I, U64, P, U64, P, P, P, P, P, I, P, P], I),
+        "parw2v_random_walks": ([P, P, I, I, I, U64, I, P], I),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -307,3 +308,18 @@ class Trainer:
                                              int(ctx_per_window), _ptr(m), _ptr(r), _ptr(k), len(m), float(h),
                                              _ptr(out)))
         return out
+
+
+def random_walks(indptr, indices, walks_per_node: int, walk_len: int, seed: int = 0, device: int = 0) -> np.ndarray:
+    """Uniform random walks over a CSR graph on the GPU (``parw2v_random_walks``): an array of
+    shape (walks_per_node * n_nodes, walk_len); walk w starts at node w mod n_nodes."""
+    lib = load_library()
+    ip = np.ascontiguousarray(indptr, dtype=np.int64)
+    ix = np.ascontiguousarray(indices, dtype=np.int32)
+    n = len(ip) - 1
+    out = np.empty((walks_per_node * n, walk_len), dtype=np.int32)
+    rc = lib.parw2v_random_walks(_ptr(ip), _ptr(ix), n, int(walks_per_node), int(walk_len), int(seed), int(device),
+                                 _ptr(out))
+    if rc:
+        raise ParW2VError(rc, lib.parw2v_last_error(None).decode())
+    return out

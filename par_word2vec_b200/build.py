@@ -21,7 +21,7 @@ BUILD = os.path.join(ROOT, "_build")
 LIB = os.path.join(HERE, "libparw2v.so")
 CLI = os.path.join(HERE, "bin", "parw2v")
 
-CU_SOURCES = ["api.cu", "k_setup.cu", "k_det.cu", "k_pack.cu", "k_plain.cu", "k_batched.cu", "k_loss.cu"]
+CU_SOURCES = ["api.cu", "k_setup.cu", "k_det.cu", "k_pack.cu", "k_plain.cu", "k_batched.cu", "k_loss.cu", "k_walks.cu"]
 CXX_SOURCES = ["frontend.cpp"]
 HEADERS = ["common.cuh", "internal.h", "mma.cuh", "sentence.cuh"]
 
