@@ -208,23 +208,26 @@ __device__ __noinline__ void merge_repeats(const int *negs, int K, const int32_t
         dup[K + r] = first;
     }
     __syncwarp();
-    for (int r = 0; r < rows; r++) {
-        const int f = dup[K + r];
-        if (f >= 0)
+    // visit only the repeated rows and negatives, in ascending order (32 at a time by ballot)
+    for (int r0 = 0; r0 < rows; r0 += 32) {
+        for (unsigned m = __ballot_sync(0xffffffffu, r0 + lane < rows && dup[K + r0 + lane] >= 0); m; m &= m - 1) {
+            const int r = r0 + __ffs(m) - 1, f = dup[K + r];
             for (int k = lane; k < K; k += 32) {
                 G[k * gs + f] += G[k * gs + r];
                 G[k * gs + r] = 0.f;
             }
-        __syncwarp();
+            __syncwarp();
+        }
     }
-    for (int k = 0; k < K; k++) {
-        const int f = dup[k];
-        if (f >= 0)
+    for (int k0 = 0; k0 < K; k0 += 32) {
+        for (unsigned m = __ballot_sync(0xffffffffu, k0 + lane < K && dup[k0 + lane] >= 0); m; m &= m - 1) {
+            const int k = k0 + __ffs(m) - 1, f = dup[k];
             for (int r = lane; r < rows; r += 32) {
                 G[f * gs + r] += G[k * gs + r];
                 G[k * gs + r] = 0.f;
             }
-        __syncwarp();
+            __syncwarp();
+        }
     }
 }
 
