@@ -102,7 +102,7 @@ __host__ __device__ inline Layout make_layout(int ld, int window, int negative, 
     const size_t g_floats = L.mma ? (size_t) kMmaK * kMmaR : (size_t) L.kmax * batch;
     L.neg_off = L.g_off + up16(g_floats * 4);
     L.dup_off = L.neg_off + up16((size_t) L.kmax * 4);
-    L.meta_off = L.dup_off + up16((size_t) (L.kmax + batch) * 4);
+    L.meta_off = L.dup_off + up16((size_t) (L.kmax + 2 * batch) * 4);
     L.ctx_off = L.meta_off + up16((size_t) L.ws * 8);
     L.exit_off = L.ctx_off + up16((size_t) (2 * window) * 8);
     L.per_warp = L.exit_off + up16((size_t) kPrefetch * 4 + 16);
@@ -190,10 +190,10 @@ struct Store<true> {  // BF16 tables
 };
 
 
-// Merge gradient rows of repeated negatives and gradient columns of repeated batch words into
-// their first occurrence (G is K x rows with row stride gs), so each distinct row is written once.
-__device__ __noinline__ void merge_repeats(const int *negs, int K, const int32_t *batch_words, int rows, float *G,
-                                              int gs, int *dup, int lane) {
+// Repeated words of a batch: dup[k] (negatives) and dup[K + r] (batch rows) get the index of the
+// word's first occurrence, or -1.  Generic form (any K, rows).
+__device__ __noinline__ void mark_repeats(const int *negs, int K, const int32_t *batch_words, int rows, int *dup,
+                                          int lane) {
     for (int k = lane; k < K; k += 32) {
         int first = -1;
         for (int q = 0; q < k && first < 0; q++)
@@ -208,7 +208,37 @@ __device__ __noinline__ void merge_repeats(const int *negs, int K, const int32_t
         dup[K + r] = first;
     }
     __syncwarp();
-    // visit only the repeated rows and negatives, in ascending order (32 at a time by ballot)
+}
+
+// The same marks for K <= 64 negatives and rows <= 32 (the tensor-core paths), by warp matching:
+// lanes holding equal words find each other in one __match_any_sync; negatives 32..63 also look
+// through the first 32 by shuffles.  Lanes without a word hold distinct negative sentinels.
+__device__ __forceinline__ void mark_repeats_small(const int *negs, int K, const int *words, int rows, int *dup,
+                                                   int lane) {
+    const int wr = lane < rows ? words[lane] : -1 - lane;
+    const unsigned mr = __match_any_sync(0xffffffffu, wr);
+    if (lane < rows) dup[K + lane] = (__ffs(mr) - 1 == lane) ? -1 : __ffs(mr) - 1;
+    const int v0 = lane < K ? negs[lane] : -1 - lane;
+    const unsigned m0 = __match_any_sync(0xffffffffu, v0);
+    if (lane < K) dup[lane] = (__ffs(m0) - 1 == lane) ? -1 : __ffs(m0) - 1;
+    if (K > 32) {
+        const int v1 = lane + 32 < K ? negs[lane + 32] : -100 - lane;
+        int first = -1;
+        for (int q = 0; q < 32; q++) {
+            const int w = __shfl_sync(0xffffffffu, v0, q);
+            if (first < 0 && q < K && w == v1) first = q;
+        }
+        const unsigned m1 = __match_any_sync(0xffffffffu, v1);
+        if (first < 0 && __ffs(m1) - 1 != lane) first = 32 + __ffs(m1) - 1;
+        if (lane + 32 < K) dup[lane + 32] = first;
+    }
+    __syncwarp();
+}
+
+// Merge the gradient columns of repeated batch rows, then the gradient rows of repeated negatives,
+// into their first occurrence (G is K x rows with row stride gs), so each distinct row is written
+// once.  Only the marked rows are visited, in ascending order (32 at a time by ballot).
+__device__ __noinline__ void merge_marked(int K, int rows, float *G, int gs, const int *dup, int lane) {
     for (int r0 = 0; r0 < rows; r0 += 32) {
         for (unsigned m = __ballot_sync(0xffffffffu, r0 + lane < rows && dup[K + r0 + lane] >= 0); m; m &= m - 1) {
             const int r = r0 + __ffs(m) - 1, f = dup[K + r];
@@ -229,6 +259,12 @@ __device__ __noinline__ void merge_repeats(const int *negs, int K, const int32_t
             __syncwarp();
         }
     }
+}
+
+__device__ __forceinline__ void merge_repeats(const int *negs, int K, const int32_t *batch_words, int rows, float *G,
+                                              int gs, int *dup, int lane) {
+    mark_repeats(negs, K, batch_words, rows, dup, lane);
+    merge_marked(K, rows, G, gs, dup, lane);
 }
 
 // Repulsion of one batch on the tensor cores (BF16 tables, K <= 48 negatives, rows <= 32).
@@ -260,6 +296,9 @@ __device__ __noinline__ void repel_mma(const TrainArgs &a, const Layout &Lo, uns
         for (int j = 0; j < 4; j++)
 #pragma unroll
             for (int e = 0; e < 4; e++) acc[i][j][e] = 0.f;
+    // the batch's words, read once: the staging and write-back loops index them per piece
+    int *sbw = dup + Lo.kmax + a.batch;
+    if (lane < rows) sbw[lane] = __ldg(bw + lane);
     __syncwarp();
 #pragma unroll 1
     for (int pass = 0; pass < 2; pass++) {
@@ -276,7 +315,7 @@ __device__ __noinline__ void repel_mma(const TrainArgs &a, const Layout &Lo, uns
                 T *dst = (rr < rows ? sin + (size_t) rr * kMmaStride : sout + (size_t) (rr - rows) * kMmaStride) + pc * 8;
                 const int col = col0 + pc * 8;
                 if (col < ld) {
-                    const T *src = (rr < rows ? w_in + (size_t) __ldg(bw + rr) * ld : w_out + (size_t) negs[rr - rows] * ld) + col;
+                    const T *src = (rr < rows ? w_in + (size_t) sbw[rr] * ld : w_out + (size_t) negs[rr - rows] * ld) + col;
                     cp_async16(dst, src);
                 } else {
                     *reinterpret_cast<uint4 *>(dst) = make_uint4(0, 0, 0, 0);
@@ -380,7 +419,7 @@ __device__ __noinline__ void repel_mma(const TrainArgs &a, const Layout &Lo, uns
                     const int col = col0 + pc * 8;
                     if (col >= ld || dup[rr < rows ? K + rr : rr - rows] >= 0) continue;
                     const T *src = (rr < rows ? sin + (size_t) rr * kMmaStride : sout + (size_t) (rr - rows) * kMmaStride) + pc * 8;
-                    T *dst = (rr < rows ? w_in + (size_t) __ldg(bw + rr) * ld : w_out + (size_t) negs[rr - rows] * ld) + col;
+                    T *dst = (rr < rows ? w_in + (size_t) sbw[rr] * ld : w_out + (size_t) negs[rr - rows] * ld) + col;
                     *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(src);
                 }
             }
@@ -394,13 +433,12 @@ __device__ __noinline__ void repel_mma(const TrainArgs &a, const Layout &Lo, uns
                 for (int nt = 0; nt < 4; nt++)
 #pragma unroll
                     for (int e = 0; e < 4; e++)
-                        if (mt < mt1 && nt < nt1)
-                            Gf[(mt * 16 + g + ((e >> 1) << 3)) * kMmaR + nt * 8 + 2 * t + (e & 1)] = acc[mt][nt][e];
-            __syncwarp();
-            for (int i = lane; i < K * kMmaR; i += 32)
-                if ((i & (kMmaR - 1)) < rows) Gf[i] = grad_from_table(Gf[i], 0, alpha, s_exp);
-            __syncwarp();
-            merge_repeats(negs, K, bw, rows, Gf, kMmaR, dup, lane);
+                        if (mt < mt1 && nt < nt1) {
+                            const int k = mt * 16 + g + ((e >> 1) << 3), r = nt * 8 + 2 * t + (e & 1);
+                            if (k < K && r < rows) Gf[k * kMmaR + r] = grad_from_table(acc[mt][nt][e], 0, alpha, s_exp);
+                        }
+            mark_repeats_small(negs, K, sbw, rows, dup, lane);
+            merge_marked(K, rows, Gf, kMmaR, dup, lane);
             for (int i = lane; i < kMmaK * (kGbStride / 2); i += 32) {
                 const int k = i / (kGbStride / 2), r = 2 * (i - k * (kGbStride / 2));
                 const float v0 = (k < K && r < rows) ? Gf[k * kMmaR + r] : 0.f;
@@ -439,6 +477,9 @@ __device__ __noinline__ void repel_mma_f32(const TrainArgs &a, const Layout &Lo,
         for (int j = 0; j < 4; j++)
 #pragma unroll
             for (int e = 0; e < 4; e++) acc[i][j][e] = 0.f;
+    // the batch's words, read once: the staging and write-back loops index them per piece
+    int *sbw = dup + Lo.kmax + a.batch;
+    if (lane < rows) sbw[lane] = __ldg(bw + lane);
     __syncwarp();
 #pragma unroll 1
     for (int pass = 0; pass < 2; pass++) {
@@ -453,7 +494,7 @@ __device__ __noinline__ void repel_mma_f32(const TrainArgs &a, const Layout &Lo,
                 float *dst = (rr < rows ? sin + (size_t) rr * kF32Stride : sout + (size_t) (rr - rows) * kF32Stride) + pc * 4;
                 const int col = col0 + pc * 4;
                 if (col < ld) {
-                    const float *src = (rr < rows ? w_in + (size_t) __ldg(bw + rr) * ld : w_out + (size_t) negs[rr - rows] * ld) + col;
+                    const float *src = (rr < rows ? w_in + (size_t) sbw[rr] * ld : w_out + (size_t) negs[rr - rows] * ld) + col;
                     cp_async16(dst, src);
                 } else {
                     *reinterpret_cast<float4 *>(dst) = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -558,7 +599,7 @@ __device__ __noinline__ void repel_mma_f32(const TrainArgs &a, const Layout &Lo,
                                     const int row = mt * 16 + g + 8 * h;
                                     if (row < rows && dup[K + row] < 0) {
                                         const float2 old = *reinterpret_cast<const float2 *>(sin + (size_t) row * kF32Stride + c);
-                                        *reinterpret_cast<float2 *>(w_in + (size_t) __ldg(bw + row) * ld + col0 + c) =
+                                        *reinterpret_cast<float2 *>(w_in + (size_t) sbw[row] * ld + col0 + c) =
                                             make_float2(old.x + q[mt][2 * h], old.y + q[mt][2 * h + 1]);
                                     }
                                 }
@@ -576,13 +617,12 @@ __device__ __noinline__ void repel_mma_f32(const TrainArgs &a, const Layout &Lo,
                 for (int nt = 0; nt < 4; nt++)
 #pragma unroll
                     for (int e = 0; e < 4; e++)
-                        if (mt < mt1 && nt < nt1)
-                            Gf[(mt * 16 + g + ((e >> 1) << 3)) * kMmaR + nt * 8 + 2 * t + (e & 1)] = acc[mt][nt][e];
-            __syncwarp();
-            for (int i = lane; i < K * kMmaR; i += 32)
-                if ((i & (kMmaR - 1)) < rows) Gf[i] = grad_from_table(Gf[i], 0, alpha, s_exp);
-            __syncwarp();
-            merge_repeats(negs, K, bw, rows, Gf, kMmaR, dup, lane);
+                        if (mt < mt1 && nt < nt1) {
+                            const int k = mt * 16 + g + ((e >> 1) << 3), r = nt * 8 + 2 * t + (e & 1);
+                            if (k < K && r < rows) Gf[k * kMmaR + r] = grad_from_table(acc[mt][nt][e], 0, alpha, s_exp);
+                        }
+            mark_repeats_small(negs, K, sbw, rows, dup, lane);
+            merge_marked(K, rows, Gf, kMmaR, dup, lane);
             for (int i = lane; i < kMmaK * kMmaR; i += 32) {
                 const int k = i / kMmaR, r = i - k * kMmaR;
                 Gp[(size_t) k * kGps + r] = (k < K && r < rows) ? Gf[i] : 0.f;
@@ -1032,7 +1072,7 @@ __host__ __device__ inline Layout make_layout_stream(int ld, int window, int neg
     const size_t g_bytes = L.mma ? 0 : up16((size_t) L.kmax * batch * 4);
     L.neg_off = L.region + g_bytes;
     L.dup_off = L.neg_off + up16((size_t) L.kmax * 4);
-    L.ctx_off = L.dup_off + up16((size_t) (L.kmax + batch) * 4);
+    L.ctx_off = L.dup_off + up16((size_t) (L.kmax + 2 * batch) * 4);
     L.exit_off = L.ctx_off + up16((size_t) (2 * window) * 8);
     L.per_warp = L.exit_off;
     return L;
