@@ -10,7 +10,7 @@ repulsion batch, sample 1e-4, batch 24, alpha 0.025, 1 iteration per step.
 A step is one training epoch over the whole corpus through the library's C ABI
 (``parw2v_train``).  ``value`` times K steps with the corpus already on the device; ``e2e``
 times K steps of the user-facing sequence set_corpus (pinned host -> device) + train +
-get_weights (W_in device -> host).  The corpus (3.2 GB) and weights exceed the 126 MB L2, so no
+get_weights (W_in device -> pinned host).  The corpus (3.2 GB) and weights exceed the 126 MB L2, so no
 L2 flush is inserted between steps.  Several GPUs run independent replicas (the training loop
 does not shard: every window updates the two shared tables); ``value`` is the words of all
 replicas over the slowest replica's time.
@@ -313,7 +313,7 @@ def main():
                 "alg_bytes_per_kept_position": alg_bytes / max(kept, 1)}
 
     # ---- end to end through the C ABI with host buffers ----
-    w_host = np.empty((V, d), np.float32)
+    w_host = torch.empty((V, d), dtype=torch.float32, pin_memory=True).numpy()  # pinned, like the corpus
 
     def e2e_step():
         tr.set_corpus(stream_np)

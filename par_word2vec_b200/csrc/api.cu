@@ -42,6 +42,8 @@ struct parw2v_ctx {
     // workspace
     float *d_scratch = nullptr;
     size_t scratch_floats = 0;
+    float *d_stage = nullptr;  // dense FP32 rows for weight copies (see copy_weights)
+    size_t stage_bytes = 0;
     DevCounters *d_cnt = nullptr;
     // trace
     parw2v_trace *trace = nullptr;
@@ -302,42 +304,46 @@ int parw2v_init_weights(parw2v_ctx *c) {
     return PARW2V_OK;
 }
 
-// Host [V][d] FP32 <-> device [V][ld] rows, through a pitched copy (and a BF16 conversion).
-static int copy_weights(parw2v_ctx *c, const float *src_h, float *dst_h, void *dev) {
+// Host [V][d] FP32 <-> device [V][ld] rows (FP32 or BF16).  The rows go through a staging buffer of
+// dense FP32 rows, at most kStageBytes, kept for later calls: one kernel converts a chunk of rows
+// between the two layouts and one linear copy moves the chunk across the host link.  (A pitched
+// copy of V rows of d floats runs at a fraction of the link's speed.)
+static constexpr size_t kStageBytes = 64ull << 20;
+
+static int copy_rows(parw2v_ctx *c, const float *src_h, float *dst_h, void *dev, bool bf16) {
     const size_t V = (size_t) c->vocab, d = (size_t) c->cfg.size, ld = (size_t) c->ld;
-    if (!c->bf16) {
+    const size_t row_bytes = sizeof(float) * d;
+    const size_t chunk = std::max<size_t>(1, std::min(V, kStageBytes / row_bytes));
+    if (c->stage_bytes < chunk * row_bytes) {
+        dfree(c, c->d_stage, c->stage_bytes);
+        c->d_stage = nullptr;
+        c->stage_bytes = 0;
+        int rc = dalloc(c, (void **) &c->d_stage, chunk * row_bytes, "weights staging");
+        if (rc) return rc;
+        c->stage_bytes = chunk * row_bytes;
+    }
+    const size_t esz = bf16 ? sizeof(__nv_bfloat16) : sizeof(float);
+    for (size_t r0 = 0; r0 < V; r0 += chunk) {
+        const size_t rows = std::min(chunk, V - r0);
+        void *drow = (char *) dev + r0 * ld * esz;
         if (src_h) {
-            CK(c, cudaMemsetAsync(dev, 0, sizeof(float) * V * ld, c->stream), "weights clear");
-            CK(c, cudaMemcpy2DAsync(dev, ld * sizeof(float), src_h, d * sizeof(float), d * sizeof(float), V,
-                                    cudaMemcpyHostToDevice, c->stream), "weights upload");
+            CK(c, cudaMemcpyAsync(c->d_stage, src_h + r0 * d, rows * row_bytes, cudaMemcpyHostToDevice, c->stream),
+               "weights upload");
+            CK(c, launch_rows_from_dense(c->d_stage, (int) d, drow, bf16, (int) ld, rows, c->stream),
+               "weights layout");
         } else {
-            CK(c, cudaMemcpy2DAsync(dst_h, d * sizeof(float), dev, ld * sizeof(float), d * sizeof(float), V,
-                                    cudaMemcpyDeviceToHost, c->stream), "weights download");
+            CK(c, launch_rows_to_dense(drow, bf16, (int) ld, c->d_stage, (int) d, rows, c->stream),
+               "weights layout");
+            CK(c, cudaMemcpyAsync(dst_h + r0 * d, c->d_stage, rows * row_bytes, cudaMemcpyDeviceToHost, c->stream),
+               "weights download");
         }
-        CK(c, cudaStreamSynchronize(c->stream), "weights copy");
-        return PARW2V_OK;
     }
-    void *tmp = nullptr;
-    const size_t bytes = sizeof(float) * V * ld;
-    int rc = dalloc(c, &tmp, bytes, "weights staging");
-    if (rc) return rc;
-    cudaError_t e = cudaSuccess;
-    if (src_h) {
-        e = cudaMemsetAsync(tmp, 0, bytes, c->stream);
-        if (e == cudaSuccess)
-            e = cudaMemcpy2DAsync(tmp, ld * sizeof(float), src_h, d * sizeof(float), d * sizeof(float), V,
-                                  cudaMemcpyHostToDevice, c->stream);
-        if (e == cudaSuccess) e = launch_narrow_bf16((float *) tmp, (__nv_bfloat16 *) dev, V * ld, c->stream);
-    } else {
-        e = launch_widen_bf16((const __nv_bfloat16 *) dev, (float *) tmp, V * ld, c->stream);
-        if (e == cudaSuccess)
-            e = cudaMemcpy2DAsync(dst_h, d * sizeof(float), tmp, ld * sizeof(float), d * sizeof(float), V,
-                                  cudaMemcpyDeviceToHost, c->stream);
-    }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-    dfree(c, tmp, bytes);
-    if (e != cudaSuccess) return cuda_fail(c, e, "weights copy");
+    CK(c, cudaStreamSynchronize(c->stream), "weights copy");
     return PARW2V_OK;
+}
+
+static int copy_weights(parw2v_ctx *c, const float *src_h, float *dst_h, void *dev) {
+    return copy_rows(c, src_h, dst_h, dev, c->bf16);
 }
 
 int parw2v_set_weights(parw2v_ctx *c, const float *w_in, const float *w_out) {
@@ -773,7 +779,7 @@ int parw2v_loss_adjoint(parw2v_ctx *c, const int32_t *tgt, const int32_t *ctxw, 
     if (rc) return rc;
     DevBatch db;
     if ((rc = upload_batch(c, tgt, ctxw, n_pairs, neg, n_neg, cpw, db))) return rc;
-    const size_t V = (size_t) c->vocab, ld = (size_t) c->ld, d = (size_t) c->cfg.size;
+    const size_t V = (size_t) c->vocab, ld = (size_t) c->ld;
     const size_t bytes = sizeof(float) * V * ld * 2;
     float *g = nullptr;
     if ((rc = dalloc(c, (void **) &g, bytes, "gradient buffers"))) {
@@ -784,17 +790,13 @@ int parw2v_loss_adjoint(parw2v_ctx *c, const int32_t *tgt, const int32_t *ctxw, 
     if (e == cudaSuccess)
         e = launch_adjoint(db.b, c->d_w_in, c->d_w_out, c->bf16, c->cfg.size, c->ld, c->d_exp, exact, g, g + V * ld,
                            c->stream);
-    if (e == cudaSuccess && d_w_in)
-        e = cudaMemcpy2DAsync(d_w_in, d * sizeof(float), g, ld * sizeof(float), d * sizeof(float), V,
-                              cudaMemcpyDeviceToHost, c->stream);
-    if (e == cudaSuccess && d_w_out)
-        e = cudaMemcpy2DAsync(d_w_out, d * sizeof(float), g + V * ld, ld * sizeof(float), d * sizeof(float), V,
-                              cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e == cudaSuccess && d_w_in) rc = copy_rows(c, nullptr, d_w_in, g, false);
+    if (e == cudaSuccess && !rc && d_w_out) rc = copy_rows(c, nullptr, d_w_out, g + V * ld, false);
     dfree(c, g, bytes);
     dfree(c, db.mem, db.bytes);
     if (e != cudaSuccess) return cuda_fail(c, e, "adjoint kernel");
-    return PARW2V_OK;
+    return rc;
 }
 
 int parw2v_loss_fd(parw2v_ctx *c, const int32_t *tgt, const int32_t *ctxw, int n_pairs, const int32_t *neg, int n_neg,

@@ -90,7 +90,9 @@ cudaError_t launch_loss_fd(const LossBatch &b, const void *w_in, const void *w_o
                            double *grad, cudaStream_t s);
 // Records the text parw2v_last_error(NULL) returns; returns code.
 int set_global_error(int code, const char *msg);
-cudaError_t launch_widen_bf16(const __nv_bfloat16 *src, float *dst, size_t n, cudaStream_t s);
-cudaError_t launch_narrow_bf16(const float *src, __nv_bfloat16 *dst, size_t n, cudaStream_t s);
+// Weight rows between the device layout (rows of ld elements, FP32 or BF16, padding zero) and dense
+// FP32 rows of d elements (the caller's layout); `rows` rows starting at the given pointers.
+cudaError_t launch_rows_to_dense(const void *dev, bool bf16, int ld, float *dst, int d, size_t rows, cudaStream_t s);
+cudaError_t launch_rows_from_dense(const float *src, int d, void *dev, bool bf16, int ld, size_t rows, cudaStream_t s);
 
 }  // namespace parw2v

@@ -142,21 +142,52 @@ cudaError_t launch_init_net(float *w_in, float *w_out, __nv_bfloat16 *b_in, __nv
     return cudaGetLastError();
 }
 
-// ---- BF16 <-> FP32 ----
-__global__ void k_widen(const __nv_bfloat16 *src, float *dst, size_t n) {
-    for (size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t) gridDim.x * blockDim.x)
-        dst[i] = __bfloat162float(src[i]);
+// ---- device rows (V x ld, FP32 or BF16, padding columns zero) <-> dense FP32 rows (V x d) ----
+// One warp per row: lanes walk the columns, so both sides are read and written coalesced.
+__device__ __forceinline__ float to_f32(float x) { return x; }
+__device__ __forceinline__ float to_f32(__nv_bfloat16 x) { return __bfloat162float(x); }
+__device__ __forceinline__ void from_f32(float x, float *p) { *p = x; }
+__device__ __forceinline__ void from_f32(float x, __nv_bfloat16 *p) { *p = __float2bfloat16_rn(x); }
+
+template <typename T>
+__global__ void k_rows_to_dense(const T *dev, int ld, float *dst, int d, size_t rows) {
+    const int lane = threadIdx.x & 31;
+    const size_t warps = (size_t) gridDim.x * (blockDim.x >> 5);
+    for (size_t r = (size_t) blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < rows; r += warps) {
+        const T *s = dev + r * (size_t) ld;
+        float *o = dst + r * (size_t) d;
+        for (int c = lane; c < d; c += 32) o[c] = to_f32(s[c]);
+    }
 }
-__global__ void k_narrow(const float *src, __nv_bfloat16 *dst, size_t n) {
-    for (size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t) gridDim.x * blockDim.x)
-        dst[i] = __float2bfloat16_rn(src[i]);
+
+template <typename T>
+__global__ void k_rows_from_dense(const float *src, int d, T *dev, int ld, size_t rows) {
+    const int lane = threadIdx.x & 31;
+    const size_t warps = (size_t) gridDim.x * (blockDim.x >> 5);
+    for (size_t r = (size_t) blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < rows; r += warps) {
+        const float *s = src + r * (size_t) d;
+        T *o = dev + r * (size_t) ld;
+        for (int c = lane; c < ld; c += 32) from_f32(c < d ? s[c] : 0.f, o + c);
+    }
 }
-cudaError_t launch_widen_bf16(const __nv_bfloat16 *src, float *dst, size_t n, cudaStream_t s) {
-    k_widen<<<148 * 8, 256, 0, s>>>(src, dst, n);
+
+static unsigned rows_grid(size_t rows) { return (unsigned) std::min<size_t>(148 * 8, (rows + 7) / 8); }
+
+cudaError_t launch_rows_to_dense(const void *dev, bool bf16, int ld, float *dst, int d, size_t rows, cudaStream_t s) {
+    if (!rows) return cudaSuccess;
+    if (bf16)
+        k_rows_to_dense<<<rows_grid(rows), 256, 0, s>>>((const __nv_bfloat16 *) dev, ld, dst, d, rows);
+    else
+        k_rows_to_dense<<<rows_grid(rows), 256, 0, s>>>((const float *) dev, ld, dst, d, rows);
     return cudaGetLastError();
 }
-cudaError_t launch_narrow_bf16(const float *src, __nv_bfloat16 *dst, size_t n, cudaStream_t s) {
-    k_narrow<<<148 * 8, 256, 0, s>>>(src, dst, n);
+
+cudaError_t launch_rows_from_dense(const float *src, int d, void *dev, bool bf16, int ld, size_t rows, cudaStream_t s) {
+    if (!rows) return cudaSuccess;
+    if (bf16)
+        k_rows_from_dense<<<rows_grid(rows), 256, 0, s>>>(src, d, (__nv_bfloat16 *) dev, ld, rows);
+    else
+        k_rows_from_dense<<<rows_grid(rows), 256, 0, s>>>(src, d, (float *) dev, ld, rows);
     return cudaGetLastError();
 }
 
