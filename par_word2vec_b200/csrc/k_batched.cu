@@ -73,6 +73,14 @@ struct Layout {  // per-warp shared-memory carve-up, in bytes (all offsets 16-by
 
 __host__ __device__ inline size_t up16(size_t x) { return (x + 15) & ~(size_t) 15; }
 
+// Head of a CTA's shared memory: the expTable (1,001 floats, padded) and 32 bytes of CTA-wide
+// constants (STREAM variant: the 2w divisor, the line count and the kept-token count), read from
+// there rather than held in registers; the warps' regions follow.
+constexpr size_t kExpBytes = 1004 * sizeof(float);
+constexpr size_t kSmemHead = kExpBytes + 32;
+static_assert(sizeof(FastMod) == 16, "the 2w divisor takes 16 of the 32 bytes");
+static_assert(kExpBytes % 16 == 0, "the constants after the expTable are 16-byte aligned");
+
 __host__ __device__ inline Layout make_layout(int ld, int window, int negative, int batch, bool bf16) {
     Layout L;
     L.ws = 2 * window + 1 + kPrefetch;
@@ -724,7 +732,7 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
     __syncthreads();
     if (wid >= warps) return;
 
-    unsigned char *base = smem_raw + up16(1004 * sizeof(float)) + (size_t) wid * Lo.per_warp;
+    unsigned char *base = smem_raw + kSmemHead + (size_t) wid * Lo.per_warp;
     float *cur = reinterpret_cast<float *>(base);                        // ws x ld FP32 (window)
     T *raw = reinterpret_cast<T *>(base + Lo.raw_off);                    // kRing x ld landing (BF16)
     T *tgt = reinterpret_cast<T *>(base + Lo.tgt_off);                    // kRing x ld target landing
@@ -1023,7 +1031,7 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
 template <int NV4, bool BF16, bool SYNC>
 cudaError_t launch_nvs(const TrainArgs &a, int grid, int warps, cudaStream_t s) {
     const Layout Lo = make_layout(a.ld, a.window, a.negative, a.batch, BF16);
-    const size_t smem = up16(1004 * sizeof(float)) + (size_t) warps * Lo.per_warp;
+    const size_t smem = kSmemHead + (size_t) warps * Lo.per_warp;
     cudaError_t e = cudaFuncSetAttribute(k_batched_train<NV4, BF16, SYNC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int) smem);
     if (e != cudaSuccess) return e;
@@ -1043,6 +1051,7 @@ cudaError_t launch_nv(const TrainArgs &a, int grid, int warps, cudaStream_t s) {
 // window ring a warp needs ~11 KB of shared memory (d = 300, window 5, 5 negatives), so more
 // sentences are in flight per SM and more of the unified L1 is left to cache rows.
 constexpr int kMaxWarpsS = 16;
+constexpr int kStreamStats = 5;  // kept, sentences, pairs, batches, negatives (per warp, in shared memory)
 constexpr size_t kStreamStage = (size_t) (kMmaR + kMmaK) * kMmaStride * 2;  // 6,400 bytes
 static_assert(kStreamStage >= (size_t) kMmaK * kMmaR * 4, "the FP32 G of pass 1 shares the staging bytes");
 
@@ -1074,7 +1083,7 @@ __host__ __device__ inline Layout make_layout_stream(int ld, int window, int neg
     L.dup_off = L.neg_off + up16((size_t) L.kmax * 4);
     L.ctx_off = L.dup_off + up16((size_t) (L.kmax + 2 * batch) * 4);
     L.exit_off = L.ctx_off + up16((size_t) (2 * window) * 8);
-    L.per_warp = L.exit_off;
+    L.per_warp = L.exit_off + up16(kStreamStats * sizeof(unsigned long long));  // the warp's statistics
     return L;
 }
 
@@ -1085,31 +1094,40 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int w = a.window, B = a.batch, ld = a.ld, d = a.d;
-    const FastMod mod_w((uint32_t) w), mod_2w((uint32_t) (2 * w));
+    const FastMod mod_w((uint32_t) w);
     const int n4 = (d + 3) >> 2;
     const Layout Lo = make_layout_stream(ld, w, a.negative, B, BF16);
     float *s_exp = reinterpret_cast<float *>(smem_raw);
+    FastMod *s_mod_2w = reinterpret_cast<FastMod *>(smem_raw + kExpBytes);
+    uint64_t *s_totals = reinterpret_cast<uint64_t *>(smem_raw + kExpBytes + sizeof(FastMod));  // lines, kept
     for (int i = threadIdx.x; i <= kExpTableSize; i += blockDim.x) s_exp[i] = a.exp_table[i];
+    if (threadIdx.x == 0) {
+        *s_mod_2w = FastMod((uint32_t) (2 * w));
+        s_totals[0] = a.cnt->n_lines;
+        s_totals[1] = a.cnt->total_kept;
+    }
     __syncthreads();
     if (wid >= warps) return;
-    unsigned char *base = smem_raw + up16(1004 * sizeof(float)) + (size_t) wid * Lo.per_warp;
+    unsigned char *base = smem_raw + kSmemHead + (size_t) wid * Lo.per_warp;
     float *G = reinterpret_cast<float *>(base + Lo.g_off);
     int *negs = reinterpret_cast<int *>(base + Lo.neg_off);
     int *dup = reinterpret_cast<int *>(base + Lo.dup_off);
     float *ctx_g = reinterpret_cast<float *>(base + Lo.ctx_off);
     int *ctx_w = reinterpret_cast<int *>(ctx_g + 2 * w);
+    // statistics live in shared memory (lane 0 adds once per sentence), not in registers
+    unsigned long long *wst = reinterpret_cast<unsigned long long *>(base + Lo.exit_off);
+    if (lane == 0)
+        for (int i = 0; i < kStreamStats; i++) wst[i] = 0;
     T *w_in = static_cast<T *>(a.w_in);
     T *w_out = static_cast<T *>(a.w_out);
-    const uint64_t n_lines = a.cnt->n_lines, total_kept = a.cnt->total_kept;
     const int epoch = hogwild_epoch(a);
-    unsigned long long st_kept = 0, st_sent = 0, st_pairs = 0, st_batches = 0, st_negs = 0;
     bool failed = false;
 
     for (;;) {
         unsigned long long line = 0;
         if (lane == 0) line = atomicAdd(&a.cnt->work, 1ULL);
         line = __shfl_sync(0xffffffffu, line, 0);
-        if (line >= n_lines || failed) break;
+        if (line >= s_totals[0] || failed) break;
         const uint32_t lo_line = line ? a.line_end[line - 1] : 0u, hi_line = a.line_end[line];
         int piece = 0;
         for (uint32_t c0 = lo_line; c0 < hi_line; c0 += kMaxSentence, piece++) {
@@ -1117,21 +1135,39 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
             const int32_t *sen = a.packed + c0;
             uint64_t rng = sentence_seed_b(a, epoch, line, piece);
             LaneBits rb{(uint32_t) mix64(rng ^ (0xA24BAED4963EE407ULL * (uint64_t) (lane + 1))) | 1u};
-            const float alpha = sentence_alpha_b(a, epoch, c0, total_kept);
+            const float alpha = sentence_alpha_b(a, epoch, c0, s_totals[1]);
+            unsigned pairs = 0, batches = 0, negs_drawn = 0;
             // ---- attraction (:529-568) ----
             // Rows are read one step ahead (the next target's row during this position, the next
-            // context's row during this pair), so the L2 latency overlaps the dependent chain.  A
-            // row read ahead that this warp writes before using it (the same word again) is
-            // replaced by the value written.
+            // context's row during this pair, and during a position's last pair the first context
+            // row of the next position), so the L2 latency overlaps the dependent chain.  A row
+            // read ahead that this warp writes before using it (the same word again) is replaced
+            // by the value written.  Each position's b is drawn one position ahead, from the same
+            // random stream, so the next position's first context is known in time.
             typename S::Raw yn[NV4];
             {
                 const T *yrow0 = w_out + (size_t) __ldg(sen) * ld;
 #pragma unroll
                 for (int k = 0; k < NV4; k++) yn[k] = lane + 32 * k < n4 ? S::loadraw_g(yrow0, lane + 32 * k) : S::zero_raw();
             }
+            rng = lcg_next(rng);
+            int b_next = (int) mod_w(rng);
+            typename S::Raw xn[NV4];
+            int c_next = 1, w_next = 0;  // position 0's first context is position 1 (its window starts at 0)
+            if constexpr (!SYNC) {
+                if (L > 1) {
+                    w_next = __ldg(sen + 1);
+                    const T *xrow0 = w_in + (size_t) w_next * ld;
+#pragma unroll
+                    for (int k = 0; k < NV4; k++) xn[k] = lane + 32 * k < n4 ? S::loadraw_g(xrow0, lane + 32 * k) : S::zero_raw();
+                }
+            }
             for (int p = 0; p < L; p++) {
-                rng = lcg_next(rng);
-                const int b = (int) mod_w(rng);
+                const int b = b_next;
+                if (p + 1 < L) {
+                    rng = lcg_next(rng);
+                    b_next = (int) mod_w(rng);
+                }
                 const int t = __ldg(sen + p);
                 T *yrow = w_out + (size_t) t * ld;
                 Row<NV4> y;
@@ -1205,15 +1241,14 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                         y.v[k] = make_float4(y.v[k].x + dy.v[k].x, y.v[k].y + dy.v[k].y, y.v[k].z + dy.v[k].z,
                                              y.v[k].w + dy.v[k].w);
                 } else if (n > 0) {
-                    // contexts c in [lo_c, hi_c] without p, in window order
-                    int c = lo_c == p ? lo_c + 1 : lo_c;
-                    int wc = __ldg(sen + c);
-                    typename S::Raw xn[NV4];
-                    {
-                        const T *xrow0 = w_in + (size_t) wc * ld;
-#pragma unroll
-                        for (int k = 0; k < NV4; k++) xn[k] = lane + 32 * k < n4 ? S::loadraw_g(xrow0, lane + 32 * k) : S::zero_raw();
-                    }
+                    // contexts c in [lo_c, hi_c] without p, in window order; the first one and its
+                    // row were read during the previous position (L > 1 gives every position one)
+                    int c = c_next;
+                    int wc = w_next;
+                    // the next position's first context: its window start, which is below it
+                    // (b_next < w), so never the position itself
+                    const bool has_next = p + 1 < L;
+                    const int c_first_next = max(p + 1 - w + b_next, 0);
                     for (int i = 0; i < n; i++) {
                         const int word = wc;
                         T *x = w_in + (size_t) word * ld;
@@ -1225,8 +1260,9 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                             f = f4_dot(xr.v[k], y.v[k], f);
                         }
                         const bool more = i + 1 < n;
-                        if (more) {
-                            c = c + 1 == p ? c + 2 : c + 1;
+                        const bool ahead = more || has_next;
+                        if (ahead) {
+                            c = more ? (c + 1 == p ? c + 2 : c + 1) : c_first_next;
                             wc = __ldg(sen + c);
                             if (wc != word) {
                                 const T *xnrow = w_in + (size_t) wc * ld;
@@ -1237,7 +1273,7 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                         }
                         f = warp_sum(f);
                         const float g = grad_from_table(f, 1, alpha, s_exp);
-                        const bool again = more && wc == word;
+                        const bool again = ahead && wc == word;
 #pragma unroll
                         for (int k = 0; k < NV4; k++) {
                             const int cc = lane + 32 * k;
@@ -1248,8 +1284,10 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                             if (again) xn[k] = r;
                         }
                     }
+                    c_next = c;
+                    w_next = wc;
                 }
-                st_pairs += n;
+                pairs += n;
 #pragma unroll
                 for (int k = 0; k < NV4; k++) {
                     const int cc = lane + 32 * k;
@@ -1265,14 +1303,14 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                 const int lo_b = nb * B;
                 const int rows = min(B, L - lo_b);
                 rng = lcg_next(rng);
-                const int rep_b = (int) ((lo_b <= w - 1 || (L - 1) - lo_b <= w - 1) ? mod_w(rng) : mod_2w(rng));
+                const int rep_b = (int) ((lo_b <= w - 1 || (L - 1) - lo_b <= w - 1) ? mod_w(rng) : (*s_mod_2w)(rng));
                 const int K = rep_b * a.negative;
                 if (!warp_draw_negatives(a.table, a.vocab, rng, sen, L, K, negs, lane, a.max_resample)) {
                     failed = true;
                     break;
                 }
-                st_batches++;
-                st_negs += K;
+                batches++;
+                negs_drawn += K;
                 if (K > 0) {
                     if constexpr (BF16) {
                         if (Lo.mma)
@@ -1288,16 +1326,21 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                 }
                 __syncwarp();
             }
-            st_kept += L;
-            st_sent++;
+            if (lane == 0) {
+                wst[0] += L;
+                wst[1] += 1;
+                wst[2] += pairs;
+                wst[3] += batches;
+                wst[4] += negs_drawn;
+            }
         }
     }
     if (lane == 0) {
-        atomicAdd(&a.cnt->kept, st_kept);
-        atomicAdd(&a.cnt->sentences, st_sent);
-        atomicAdd(&a.cnt->pairs, st_pairs);
-        atomicAdd(&a.cnt->batches, st_batches);
-        atomicAdd(&a.cnt->negatives, st_negs);
+        atomicAdd(&a.cnt->kept, wst[0]);
+        atomicAdd(&a.cnt->sentences, wst[1]);
+        atomicAdd(&a.cnt->pairs, wst[2]);
+        atomicAdd(&a.cnt->batches, wst[3]);
+        atomicAdd(&a.cnt->negatives, wst[4]);
         if (failed) atomicOr(&a.cnt->error, kErrResample);
     }
 }
@@ -1305,7 +1348,7 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
 template <int NV4, bool BF16, bool SYNC>
 cudaError_t launch_stream_nvs(const TrainArgs &a, int grid, int warps, cudaStream_t s) {
     const Layout Lo = make_layout_stream(a.ld, a.window, a.negative, a.batch, BF16);
-    const size_t smem = up16(1004 * sizeof(float)) + (size_t) warps * Lo.per_warp;
+    const size_t smem = kSmemHead + (size_t) warps * Lo.per_warp;
     cudaError_t e = cudaFuncSetAttribute(k_stream_train<NV4, BF16, SYNC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
     if (e != cudaSuccess) return e;
     k_stream_train<NV4, BF16, SYNC><<<grid, warps * 32, smem, s>>>(a, warps);
@@ -1340,7 +1383,7 @@ cudaError_t launch_mode(const TrainArgs &a, int grid, int warps, cudaStream_t s)
 int batched_max_warps(int ld, int window, int negative, int batch, bool bf16, size_t *per_warp, bool stream) {
     const Layout Lo = stream ? make_layout_stream(ld, window, negative, batch, bf16) : make_layout(ld, window, negative, batch, bf16);
     if (per_warp) *per_warp = Lo.per_warp;
-    const size_t avail = kSmemBudget - up16(1004 * sizeof(float));
+    const size_t avail = kSmemBudget - kSmemHead;
     long w = (long) (avail / Lo.per_warp);
     const long cap = stream ? kMaxWarpsS : kMaxWarpsB;
     if (w > cap) w = cap;
