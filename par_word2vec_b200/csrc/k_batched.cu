@@ -310,10 +310,16 @@ __device__ __noinline__ void repel_mma(const TrainArgs &a, const Layout &Lo, uns
     __syncwarp();
 #pragma unroll 1
     for (int pass = 0; pass < 2; pass++) {
-        // zero the staging: padding rows stay zero for every chunk of the pass (the FP32 G of
-        // pass 1 may share these bytes, see the streamed kernel)
-        for (int i = lane; i < (kMmaR + kMmaK) * kMmaStride / 8; i += 32)
-            reinterpret_cast<uint4 *>(sin)[i] = make_uint4(0, 0, 0, 0);
+        // zero the padding rows the products read (batch rows up to kMmaR, negatives up to the
+        // m-tile), columns 0..kMmaCols-1; they stay zero for every chunk of the pass, since the
+        // staging writes only the real rows (the FP32 G of pass 1 may share these bytes, see the
+        // streamed kernel, so pass 2 zeroes them again)
+        const int pad_in = kMmaR - rows, pad_out = 16 * mt1 - K;
+        for (int i = lane; i < (pad_in + pad_out) * kPieces; i += 32) {
+            const int pr = i / kPieces, q = i - pr * kPieces;
+            T *row = pr < pad_in ? sin + (size_t) (rows + pr) * kMmaStride : sout + (size_t) (K + pr - pad_in) * kMmaStride;
+            reinterpret_cast<uint4 *>(row)[q] = make_uint4(0, 0, 0, 0);
+        }
         __syncwarp();
 #pragma unroll 1
         for (int col0 = 0; col0 < ld; col0 += kMmaCols) {
@@ -447,11 +453,13 @@ __device__ __noinline__ void repel_mma(const TrainArgs &a, const Layout &Lo, uns
                         }
             mark_repeats_small(negs, K, sbw, rows, dup, lane);
             merge_marked(K, rows, Gf, kMmaR, dup, lane);
-            for (int i = lane; i < kMmaK * (kGbStride / 2); i += 32) {
-                const int k = i / (kGbStride / 2), r = 2 * (i - k * (kGbStride / 2));
+            // BF16 G over the part pass 2 reads: negatives below 16 * mt1, batch rows below 16 * kr
+            const int sh = kr == 1 ? 3 : 4;  // column pairs per row: 8 * kr
+            for (int i = lane; i < (16 * mt1) << sh; i += 32) {
+                const int k = i >> sh, r = 2 * (i & ((1 << sh) - 1));
                 const float v0 = (k < K && r < rows) ? Gf[k * kMmaR + r] : 0.f;
                 const float v1 = (k < K && r + 1 < rows) ? Gf[k * kMmaR + r + 1] : 0.f;
-                reinterpret_cast<__nv_bfloat162 *>(Gb)[i] = __floats2bfloat162_rn(v0, v1);
+                reinterpret_cast<__nv_bfloat162 *>(Gb + (size_t) k * kGbStride)[r >> 1] = __floats2bfloat162_rn(v0, v1);
             }
             __syncwarp();
         }

@@ -19,7 +19,9 @@ __device__ __forceinline__ unsigned pack_sr2(float2 v, uint64_t h) {
 
 // Per-lane stream of random bits for stochastic rounding: a 32-bit LCG (multiplier 747796405,
 // increment 2891336453) with its high half folded into the low half, so both 16-bit fields of a
-// word carry high-order bits; two steps give the four fields one float4 write-back needs.
+// word carry high-order bits.  One step serves the four values of a float4 write-back: the second
+// pair takes the word with its halves swapped, so each value still sees a uniform 16-bit field
+// (each rounding stays unbiased; values 0 and 3, 1 and 2 share a field).
 struct LaneBits {
     uint32_t s;
     __device__ __forceinline__ uint32_t step() {
@@ -28,7 +30,7 @@ struct LaneBits {
     }
     __device__ __forceinline__ uint64_t next() {
         const uint32_t lo = step();
-        return ((uint64_t) step() << 32) | lo;
+        return ((uint64_t) __funnelshift_l(lo, lo, 16) << 32) | lo;
     }
 };
 
