@@ -1148,10 +1148,12 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
             // ---- attraction (:529-568) ----
             // Rows are read one step ahead (the next target's row during this position, the next
             // context's row during this pair, and during a position's last pair the first context
-            // row of the next position), so the L2 latency overlaps the dependent chain.  A row
-            // read ahead that this warp writes before using it (the same word again) is replaced
-            // by the value written.  Each position's b is drawn one position ahead, from the same
-            // random stream, so the next position's first context is known in time.
+            // row of the next position; BF16 tables only), so the L2 latency overlaps the
+            // dependent chain.  A row read ahead that this warp writes before using it (the same
+            // word again) is replaced by the value written.  Each position's b is drawn one
+            // position ahead, from the same random stream, so the next position's first context
+            // is known in time.  With FP32 tables the raw row is twice the registers, and keeping
+            // it across positions measured 5% slower: there a position reads its first row itself.
             typename S::Raw yn[NV4];
             {
                 const T *yrow0 = w_out + (size_t) __ldg(sen) * ld;
@@ -1162,7 +1164,7 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
             int b_next = (int) mod_w(rng);
             typename S::Raw xn[NV4];
             int c_next = 1, w_next = 0;  // position 0's first context is position 1 (its window starts at 0)
-            if constexpr (!SYNC) {
+            if constexpr (!SYNC && BF16) {
                 if (L > 1) {
                     w_next = __ldg(sen + 1);
                     const T *xrow0 = w_in + (size_t) w_next * ld;
@@ -1253,6 +1255,13 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                     // row were read during the previous position (L > 1 gives every position one)
                     int c = c_next;
                     int wc = w_next;
+                    if constexpr (!BF16) {
+                        c = lo_c == p ? lo_c + 1 : lo_c;
+                        wc = __ldg(sen + c);
+                        const T *xrow0 = w_in + (size_t) wc * ld;
+#pragma unroll
+                        for (int k = 0; k < NV4; k++) xn[k] = lane + 32 * k < n4 ? S::loadraw_g(xrow0, lane + 32 * k) : S::zero_raw();
+                    }
                     // the next position's first context: its window start, which is below it
                     // (b_next < w), so never the position itself
                     const bool has_next = p + 1 < L;
@@ -1268,7 +1277,7 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                             f = f4_dot(xr.v[k], y.v[k], f);
                         }
                         const bool more = i + 1 < n;
-                        const bool ahead = more || has_next;
+                        const bool ahead = more || (BF16 && has_next);
                         if (ahead) {
                             c = more ? (c + 1 == p ? c + 2 : c + 1) : c_first_next;
                             wc = __ldg(sen + c);
