@@ -133,7 +133,10 @@ int parw2v_get_exp_table(parw2v_ctx *ctx, float *exp_table);
 /* InitNet (cpu.cpp:337-357) on the device: W_in from the seed-1 LCG, W_out = 0. */
 int parw2v_init_weights(parw2v_ctx *ctx);
 /* Host <-> device copies of the vocab_size x size row-major FP32 matrices (either may be
- * NULL).  In BF16 mode set_weights rounds to nearest and get_weights widens exactly. */
+ * NULL).  In BF16 mode set_weights rounds to nearest and get_weights widens exactly.  The
+ * rows pass through a device staging buffer of at most 64 MiB, allocated on first use, kept
+ * by the context and counted against mem_cap_bytes.  Host buffers may be pageable; pinned
+ * buffers (cudaHostAlloc) move at the full host-link speed. */
 int parw2v_set_weights(parw2v_ctx *ctx, const float *w_in, const float *w_out);
 int parw2v_get_weights(parw2v_ctx *ctx, float *w_in, float *w_out);
 
