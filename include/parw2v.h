@@ -66,7 +66,22 @@ typedef struct {
                         min_rounds; < 0: no cap */
     int attraction;  /* PARW2V_ATTRACT_*: how the contexts of one target are applied */
     int variant;     /* BATCHED modes: PARW2V_VARIANT_* kernel organisation */
+    int staging;     /* BATCHED modes: PARW2V_STAGING_* copies of the repulsion's rows into
+                        shared memory */
+    int autotune;    /* BATCHED modes: 1 = on the first parw2v_train (and whenever the number of
+                        sentences in flight changes), time short trials of the launch knobs that
+                        do not change the result -- the split of the sentences in flight into CTAs
+                        and warps, the row elements per lane of the streamed kernel and the staging
+                        copies (unless cfg.staging fixes it) -- on a prefix of the first epoch, with
+                        the weights restored after each trial, and keep the fastest; 0 = the
+                        compiled-in choices */
 } parw2v_config;
+
+/* Repulsion staging of the BATCHED modes (cfg.staging); the result does not depend on it */
+#define PARW2V_STAGING_AUTO 0     /* BULK */
+#define PARW2V_STAGING_BULK 1     /* one bulk copy (cp.async.bulk, the TMA unit) per row and column
+                                     chunk, completing on a shared-memory mbarrier */
+#define PARW2V_STAGING_CPASYNC 2  /* 16-byte cp.async copies */
 
 /* Kernel organisation of the BATCHED modes (cfg.variant) */
 #define PARW2V_VARIANT_AUTO 0    /* STREAM */
@@ -94,7 +109,18 @@ typedef struct {
     double kernel_ms;    /* device time of the training kernels (CUDA events) */
     double pack_ms;      /* device time of subsampling + packing (Hogwild modes) */
     float final_alpha;   /* learning rate at the end */
+    int grid;            /* Hogwild modes: persistent CTAs of the training kernel's launch */
+    int warps_per_cta;   /* Hogwild modes: sentences in flight per CTA */
+    int repulsion;       /* PARW2V_REPULSION_* path the training kernel took for the batches */
+    int lane_elems;      /* BATCHED streamed kernel: row elements each lane holds */
+    int staging;         /* BATCHED modes: PARW2V_STAGING_BULK or _CPASYNC as launched */
 } parw2v_stats;
+
+/* parw2v_stats.repulsion */
+#define PARW2V_REPULSION_SERIAL 0   /* DET and PLAIN: the reference's three products in order */
+#define PARW2V_REPULSION_TENSOR 1   /* BATCHED: warp-level tensor-core products (batch <= 32 rows,
+                                       (2*window-1)*negative <= 96 negatives) */
+#define PARW2V_REPULSION_CUDA 2     /* BATCHED: CUDA-core products (larger batches) */
 
 /* Deterministic-mode trace: the random decisions of the run, for parity checks. Host
  * buffers; an entry beyond a capacity is counted but not stored. */
@@ -112,7 +138,8 @@ typedef struct parw2v_ctx parw2v_ctx;
 /* Library identification and error text. */
 const char *parw2v_version(void);
 const char *parw2v_strerror(int status);
-/* Detail of the last error on this context (or of the last failed create when ctx is NULL). */
+/* Detail of the last error on this context.  With ctx NULL: the calling thread's last error of a
+ * call that has no context (parw2v_create, parw2v_det_train_noalloc, parw2v_random_walks). */
 const char *parw2v_last_error(const parw2v_ctx *ctx);
 
 /* Replaces the globals set by main() + the device set-up of gpu_text.cu:1090-1100.
@@ -203,9 +230,11 @@ int parw2v_random_walks(const int64_t *indptr, const int32_t *indices, int n_nod
  *   d_w_in/out   vocab_size rows of ld floats, trained in place
  *   stream       a cudaStream_t (NULL = the default stream); the call returns after the stream
  *                has finished the training, with stats filled (may be NULL)
- * cfg.device selects the GPU (made current for the call).  The first call on a device looks up
- * the array's device address; make that first call before any stream capture.  All calls share
- * the one array, so calls that overlap on the same GPU race: serialise them. */
+ * cfg.device selects the GPU (made current for the call).  Each call looks up the array's device
+ * address in the current context, clears the counters at the array's start and waits for the
+ * stream: the call is synchronous, and must not be made while its stream is being captured.  All
+ * calls share the one array and it keeps the last call's contents, so calls that overlap on the
+ * same GPU (from several threads or several streams) race: serialise them. */
 int parw2v_det_train_noalloc(const parw2v_config *cfg, int vocab_size, uint64_t train_words,
                              const int32_t *d_corpus, uint64_t n_tokens, const int32_t *d_table,
                              const float *d_exp_table, const float *d_keep_thr, float *d_w_in,

@@ -25,6 +25,8 @@ EXP_TABLE_SIZE = 1000
 
 ATTRACT_DEFAULT, ATTRACT_SEQUENTIAL, ATTRACT_WINDOW = 0, 1, 2
 VARIANT_AUTO, VARIANT_WINDOW, VARIANT_STREAM = 0, 1, 2
+STAGING_AUTO, STAGING_BULK, STAGING_CPASYNC = 0, 1, 2
+REPULSION_SERIAL, REPULSION_TENSOR, REPULSION_CUDA = 0, 1, 2
 OK, ERR_ARG, ERR_CUDA, ERR_OOM, ERR_CAPACITY, ERR_TIMEOUT, ERR_STATE, ERR_IO, ERR_NODEV = 0, -1, -2, -3, -4, -5, -6, -7, -8
 
 # every symbol include/parw2v.h declares (checked by tests against the built library)
@@ -51,13 +53,15 @@ class Config(ctypes.Structure):
                 ("sample", ctypes.c_float), ("mode", ctypes.c_int), ("device", ctypes.c_int),
                 ("seed", ctypes.c_uint64), ("grid", ctypes.c_int), ("warps_per_cta", ctypes.c_int),
                 ("mem_cap_bytes", ctypes.c_size_t), ("min_rounds", ctypes.c_int), ("attraction", ctypes.c_int),
-                ("variant", ctypes.c_int)]
+                ("variant", ctypes.c_int), ("staging", ctypes.c_int), ("autotune", ctypes.c_int)]
 
 
 class _Stats(ctypes.Structure):
     _fields_ = [("words", ctypes.c_uint64), ("kept", ctypes.c_uint64), ("sentences", ctypes.c_uint64),
                 ("pairs", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("negatives", ctypes.c_uint64),
-                ("kernel_ms", ctypes.c_double), ("pack_ms", ctypes.c_double), ("final_alpha", ctypes.c_float)]
+                ("kernel_ms", ctypes.c_double), ("pack_ms", ctypes.c_double), ("final_alpha", ctypes.c_float),
+                ("grid", ctypes.c_int), ("warps_per_cta", ctypes.c_int), ("repulsion", ctypes.c_int),
+                ("lane_elems", ctypes.c_int), ("staging", ctypes.c_int)]
 
 
 class _Trace(ctypes.Structure):
@@ -184,13 +188,14 @@ class Trainer:
 
     def __init__(self, size=100, window=5, negative=5, batch_size=24, iter=5, alpha=0.025, sample=1e-3,
                  mode=MODE_BATCHED_BF16, device=0, seed=0, grid=0, warps_per_cta=0, mem_cap_bytes=0, min_rounds=0, attraction=0,
-                 variant=0):
+                 variant=0, staging=0, autotune=0):
         self._lib = load_library()
         if isinstance(mode, str):
             mode = MODE_NAMES[mode]
         self.cfg = Config(int(size), int(window), int(negative), int(batch_size), int(iter), float(alpha),
                           float(sample), int(mode), int(device), int(seed), int(grid), int(warps_per_cta),
-                          int(mem_cap_bytes), int(min_rounds), int(attraction), int(variant))
+                          int(mem_cap_bytes), int(min_rounds), int(attraction), int(variant), int(staging),
+                          int(autotune))
         self._h = ctypes.c_void_p()
         rc = self._lib.parw2v_create(ctypes.byref(self.cfg), ctypes.byref(self._h))
         if rc:

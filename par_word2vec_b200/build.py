@@ -23,7 +23,7 @@ CLI = os.path.join(HERE, "bin", "parw2v")
 
 CU_SOURCES = ["api.cu", "k_setup.cu", "k_det.cu", "k_pack.cu", "k_plain.cu", "k_batched.cu", "k_loss.cu", "k_walks.cu"]
 CXX_SOURCES = ["frontend.cpp"]
-HEADERS = ["common.cuh", "internal.h", "mma.cuh", "sentence.cuh"]
+HEADERS = ["common.cuh", "internal.h", "mma.cuh", "sentence.cuh", "bulk.cuh", "repel.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",

@@ -7,6 +7,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "common.cuh"
 #include "internal.h"
 
@@ -51,9 +53,31 @@ struct parw2v_ctx {
     size_t trace_bytes = 0;
     void *d_trace_mem = nullptr;
     int last_grid = 0, last_warps = 0;  // launch shape of the last Hogwild training call
+    bool corpus_checked = false;        // the corpus's ids were validated against this vocabulary
+    // the two epoch graphs (packing; training + epoch advance) of the last Hogwild call, kept for
+    // the next call with the same launch arguments
+    cudaGraphExec_t graphs[2] = {nullptr, nullptr};
+    TrainArgs graph_args{};
+    int graph_grid = 0, graph_warps = 0;
+    // launch knobs chosen by the autotuner (cfg.autotune) for `inflight` sentences in flight
+    struct {
+        bool done = false;
+        uint64_t inflight = 0;
+        int grid = 0, warps = 0, stage_bulk = 1, lane_elems = 0;
+    } tuned;
 };
 
-static std::string g_create_error;
+static void drop_graphs(parw2v_ctx *c) {
+    for (auto &g : c->graphs)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
+// Text of the last error not tied to a context (a failed create, the allocation-free entry point,
+// the random walks), per calling thread: calls on different threads never share it.
+static thread_local std::string g_create_error;
 
 namespace parw2v {
 int set_global_error(int code, const char *msg) {
@@ -148,6 +172,8 @@ int parw2v_create(const parw2v_config *cfg, parw2v_ctx **out) {
         return fail(nullptr, PARW2V_ERR_ARG, "invalid kernel variant");
     if (k.attraction < PARW2V_ATTRACT_DEFAULT || k.attraction > PARW2V_ATTRACT_WINDOW)
         return fail(nullptr, PARW2V_ERR_ARG, "invalid attraction variant");
+    if (k.staging < PARW2V_STAGING_AUTO || k.staging > PARW2V_STAGING_CPASYNC)
+        return fail(nullptr, PARW2V_ERR_ARG, "invalid staging method");
     if (k.window > 100 || k.negative > 100 || k.batch_size > 1000)
         return fail(nullptr, PARW2V_ERR_CAPACITY, "window/negative/batch_size beyond the supported range");
     if (k.mode != PARW2V_MODE_DET && k.size > 512)
@@ -161,7 +187,9 @@ int parw2v_create(const parw2v_config *cfg, parw2v_ctx **out) {
     parw2v_ctx *c = new parw2v_ctx();
     c->cfg = k;
     c->bf16 = (k.mode == PARW2V_MODE_BATCHED_BF16);
-    const int align = c->bf16 ? 8 : 4;  // 16-byte rows
+    // rows of whole 32-byte sectors: every column chunk of the repulsion is a whole number of
+    // tensor-core k-steps, and a row starts on a sector
+    const int align = c->bf16 ? 16 : 8;
     c->ld = (k.size + align - 1) / align * align;
     int rc = set_device(c);
     if (rc == PARW2V_OK) {
@@ -202,6 +230,7 @@ void parw2v_destroy(parw2v_ctx *c) {
     if (!c) return;
     cudaSetDevice(c->cfg.device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    drop_graphs(c);
     for (void *p : c->owned) cudaFree(p);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -235,6 +264,7 @@ int parw2v_set_vocab(parw2v_ctx *c, const uint32_t *counts, int V) {
     uint64_t tw = 0;
     for (int i = 0; i < V; i++) tw += counts[i];
     c->train_words = tw;
+    c->corpus_checked = false;
     // cn^0.75 as the reference computes it: pow(unsigned, float) promotes both to double
     std::vector<double> pw((size_t) V);
     for (int i = 0; i < V; i++) pw[(size_t) i] = pow((double) counts[i], (double) 0.75f);
@@ -385,6 +415,7 @@ int parw2v_set_corpus(parw2v_ctx *c, const int32_t *tokens, uint64_t n) {
     if (n) CK(c, cudaMemcpyAsync(c->d_corpus, tokens, sizeof(int32_t) * n, cudaMemcpyHostToDevice, c->stream), "corpus upload");
     CK(c, cudaMemsetAsync(c->d_corpus + n, 0, sizeof(int32_t) * 16, c->stream), "sentinel");
     c->n_tokens = n;
+    c->corpus_checked = false;
     return PARW2V_OK;
 }
 
@@ -548,6 +579,98 @@ static uint64_t hogwild_cap(int min_rounds, uint64_t n_lines, uint64_t n_tokens)
     return std::max<uint64_t>(std::max<uint64_t>(1, 7000 / per_line), n_lines / 8192);
 }
 
+// The autotuner (cfg.autotune): short timed trials of the BATCHED launch knobs that leave the
+// result unchanged -- how the sentences in flight split into CTAs and warps (their number stays),
+// the row elements per lane of the streamed kernel, the staging copies -- each on a prefix of the
+// first epoch's packed corpus, after a warm launch, with the weights and counters restored after
+// every launch.  The fastest is kept in the context.  Returns an error only for a failed CUDA call;
+// without the memory for the weight backup it keeps the compiled-in choices.
+static int autotune(parw2v_ctx *c, TrainArgs a, int base_grid, int base_warps) {
+    const bool stream = stream_variant(c);
+    const parw2v_config &k = c->cfg;
+    c->tuned = {};
+    struct Cand {
+        int grid, warps, bulk, elems;
+    };
+    std::vector<std::pair<int, int>> splits = {{base_grid, base_warps}};
+    for (int f : {2, 4})
+        if (base_warps % f == 0 &&
+            batched_ctas_per_sm(c->ld, k.window, k.negative, k.batch_size, c->bf16, stream, base_warps / f) >= f)
+            splits.push_back({base_grid * f, base_warps / f});
+    std::vector<int> elems = {0};
+    if (stream) {
+        const int e0 = stream_lane_elems_default(k.size), e1 = stream_lane_elems_next(e0);
+        elems = {e0};
+        if (e1) elems.push_back(e1);
+    }
+    std::vector<int> bulks;
+    if (k.staging != PARW2V_STAGING_AUTO) bulks = {k.staging != PARW2V_STAGING_CPASYNC ? 1 : 0};
+    else if (batched_tensor_repulsion(k.window, k.negative, k.batch_size)) bulks = {1, 0};
+    else bulks = {1};
+    std::vector<Cand> cands;
+    for (auto &sp : splits)
+        for (int e : elems)
+            for (int b : bulks) cands.push_back({sp.first, sp.second, b, e});
+    // epoch 0's packed corpus
+    CK(c, cudaMemsetAsync(&c->d_cnt->work, 0, sizeof(unsigned long long), c->stream), "autotune");
+    CK(c, launch_pack(a, c->d_packed, c->d_line_end, c->d_tile_kept, c->d_tile_zero, pack_tiles(c->n_tokens), c->stream),
+       "autotune packing");
+    DevCounters h0;
+    int rc = read_counters(c, &h0);
+    if (rc) return rc;
+    const uint64_t inflight = (uint64_t) base_grid * base_warps;
+    if (h0.n_lines == 0 || cands.size() < 2) return PARW2V_OK;
+    const uint64_t trial = std::min<uint64_t>(h0.n_lines, std::max<uint64_t>(h0.n_lines / 50, 8 * inflight));
+    const uint64_t warm = std::min<uint64_t>(h0.n_lines, inflight);
+    const size_t wbytes = welem(c) * (size_t) c->vocab * c->ld;
+    void *backup = nullptr;
+    if (dalloc(c, &backup, 2 * wbytes, "autotune weight backup") != PARW2V_OK) {
+        c->err.clear();
+        return PARW2V_OK;
+    }
+    auto copy = [&](void *dst, const void *src) {
+        return cudaMemcpyAsync(dst, src, wbytes, cudaMemcpyDeviceToDevice, c->stream);
+    };
+    cudaError_t e = copy(backup, c->d_w_in);
+    if (e == cudaSuccess) e = copy((char *) backup + wbytes, c->d_w_out);
+    float best_ms = 0.f;
+    Cand best = cands[0];
+    for (size_t i = 0; i < cands.size() && e == cudaSuccess; i++) {
+        const Cand &cd = cands[i];
+        a.stage_bulk = cd.bulk;
+        a.lane_elems = cd.elems;
+        float ms = 0.f;
+        for (int pass = 0; pass < 2 && e == cudaSuccess; pass++) {
+            DevCounters hc = h0;
+            hc.n_lines = pass == 0 ? warm : trial;
+            hc.work = 0;
+            e = cudaMemcpyAsync(c->d_cnt, &hc, sizeof(hc), cudaMemcpyHostToDevice, c->stream);
+            if (e == cudaSuccess) e = cudaEventRecord(c->ev0, c->stream);
+            if (e == cudaSuccess) e = launch_batched_train(a, c->bf16, stream, cd.grid, cd.warps, c->stream);
+            if (e == cudaSuccess) e = cudaEventRecord(c->ev1, c->stream);
+            if (e == cudaSuccess) e = copy(c->d_w_in, backup);
+            if (e == cudaSuccess) e = copy(c->d_w_out, (char *) backup + wbytes);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+            if (e == cudaSuccess && pass == 1) e = cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        }
+        if (e == cudaSuccess && (i == 0 || ms < best_ms)) {
+            best_ms = ms;
+            best = cd;
+        }
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c->d_cnt, &h0, sizeof(h0), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    dfree(c, backup, 2 * wbytes);
+    if (e != cudaSuccess) return cuda_fail(c, e, "autotune trials");
+    c->tuned.done = true;
+    c->tuned.inflight = inflight;
+    c->tuned.grid = best.grid;
+    c->tuned.warps = best.warps;
+    c->tuned.stage_bulk = best.bulk;
+    c->tuned.lane_elems = best.elems;
+    return PARW2V_OK;
+}
+
 static int train_hogwild(parw2v_ctx *c, TrainArgs &a, parw2v_stats *st) {
     int rc = ensure_packing(c);
     if (rc) return rc;
@@ -587,15 +710,31 @@ static int train_hogwild(parw2v_ctx *c, TrainArgs &a, parw2v_stats *st) {
             grid = (int) std::min<uint64_t>((uint64_t) std::min(grid, sms), std::max<uint64_t>(1, cap / (uint64_t) warps));
         }
     }
+    if (!plain && c->cfg.autotune) {
+        const uint64_t inflight = (uint64_t) grid * warps;
+        if (!c->tuned.done || c->tuned.inflight != inflight) {
+            if ((rc = autotune(c, a, grid, warps))) return rc;
+        }
+        if (c->tuned.done && c->tuned.inflight == inflight) {
+            grid = c->tuned.grid;
+            warps = c->tuned.warps;
+            a.stage_bulk = c->tuned.stage_bulk;
+            a.lane_elems = c->tuned.lane_elems;
+        }
+    }
     c->last_grid = grid;
     c->last_warps = warps;
     // One epoch is two CUDA graphs, captured once and replayed for every epoch: (reset the work
     // counter, subsample and pack) and (train, advance the epoch index in device memory).  The
     // timing events are recorded between the two launches, outside the graphs.
     CK(c, cudaMemsetAsync(&c->d_cnt->epoch, 0, sizeof(unsigned), c->stream), "counters");
-    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    // the graphs of the previous call serve again when every launch argument is the same
+    const bool reuse = c->graphs[0] && c->graphs[1] && grid == c->graph_grid && warps == c->graph_warps &&
+                       memcmp(&a, &c->graph_args, sizeof(TrainArgs)) == 0;
+    if (!reuse) drop_graphs(c);
+    cudaGraphExec_t *exec = c->graphs;
     cudaError_t e = cudaSuccess;
-    for (int part = 0; part < 2 && e == cudaSuccess; part++) {
+    for (int part = 0; part < 2 && e == cudaSuccess && !reuse; part++) {
         cudaGraph_t graph = nullptr;
         e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) break;
@@ -614,24 +753,25 @@ static int train_hogwild(parw2v_ctx *c, TrainArgs &a, parw2v_stats *st) {
         if (e == cudaSuccess) e = cudaGraphInstantiate(&exec[part], graph, 0);
         if (graph) cudaGraphDestroy(graph);
     }
-    auto release = [&]() {
-        for (auto &x : exec)
-            if (x) cudaGraphExecDestroy(x);
-    };
     if (e != cudaSuccess) {
-        release();
+        drop_graphs(c);
         return cuda_fail(c, e, "capturing the epoch graphs");
     }
+    c->graph_args = a;
+    c->graph_grid = grid;
+    c->graph_warps = warps;
     float pack_ms_total = 0.f, kernel_ms_total = 0.f;
     for (int ep = 0; ep < c->cfg.iter; ep++) {
+        nvtxRangePushA("parw2v epoch");
         e = cudaEventRecord(c->ev0, c->stream);
         if (e == cudaSuccess) e = cudaGraphLaunch(exec[0], c->stream);
         if (e == cudaSuccess) e = cudaEventRecord(c->ev1, c->stream);
         if (e == cudaSuccess) e = cudaGraphLaunch(exec[1], c->stream);
         if (e == cudaSuccess) e = cudaEventRecord(c->ev2, c->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        nvtxRangePop();
         if (e != cudaSuccess) {
-            release();
+            drop_graphs(c);
             return cuda_fail(c, e, "training epoch");
         }
         float m0 = 0, m1 = 0;
@@ -640,7 +780,6 @@ static int train_hogwild(parw2v_ctx *c, TrainArgs &a, parw2v_stats *st) {
         pack_ms_total += m0;
         kernel_ms_total += m1;
     }
-    release();
     DevCounters h;
     if ((rc = read_counters(c, &h))) return rc;
     if (st) {
@@ -652,8 +791,23 @@ static int train_hogwild(parw2v_ctx *c, TrainArgs &a, parw2v_stats *st) {
         st->negatives = h.negatives;
         st->kernel_ms = kernel_ms_total;
         st->pack_ms = pack_ms_total;
-        st->final_alpha = c->cfg.alpha * 0.0001f;
+        // the schedule's rate after all epochs (the kernels' per-sentence rate at the end of the
+        // last epoch), floored at alpha * 1e-4 (PAR_Word2Vec_cpu.cpp:437-445)
+        const double done = (double) c->cfg.iter * (double) c->n_tokens;
+        const float end_alpha =
+            c->cfg.alpha * (float) (1.0 - done / ((double) c->cfg.iter * (double) c->train_words + 1.0));
+        st->final_alpha = std::max(end_alpha, c->cfg.alpha * 0.0001f);
+        st->grid = grid;
+        st->warps_per_cta = warps;
+        st->lane_elems = plain ? 0 : (a.lane_elems ? a.lane_elems : (stream_variant(c) ? stream_lane_elems_default(c->cfg.size) : 0));
+        st->staging = plain ? 0 : (a.stage_bulk ? PARW2V_STAGING_BULK : PARW2V_STAGING_CPASYNC);
+        st->repulsion = plain ? PARW2V_REPULSION_SERIAL
+                              : (batched_tensor_repulsion(c->cfg.window, c->cfg.negative, c->cfg.batch_size)
+                                     ? PARW2V_REPULSION_TENSOR
+                                     : PARW2V_REPULSION_CUDA);
     }
+    if (h.error & kErrStaging)
+        return fail(c, PARW2V_ERR_TIMEOUT, "a bulk copy of the repulsion's rows did not complete in time");
     if (h.error & kErrResample)
         return fail(c, PARW2V_ERR_TIMEOUT, "negative resampling exceeded its draw limit (every word is in the sentence?)");
     return PARW2V_OK;
@@ -668,15 +822,21 @@ int parw2v_train(parw2v_ctx *c, parw2v_stats *st) {
     int rc = set_device(c);
     if (rc) return rc;
     CK(c, cudaMemsetAsync(c->d_cnt, 0, sizeof(DevCounters), c->stream), "counters");
-    if (c->n_tokens) {
-        k_validate<<<148 * 4, 256, 0, c->stream>>>(c->d_corpus, c->n_tokens, c->vocab, c->d_cnt);
-        CK(c, cudaGetLastError(), "validation kernel");
+    if (!c->corpus_checked) {
+        // ids against the vocabulary and the count of lines: once per corpus and vocabulary
+        if (c->n_tokens) {
+            k_validate<<<148 * 4, 256, 0, c->stream>>>(c->d_corpus, c->n_tokens, c->vocab, c->d_cnt);
+            CK(c, cudaGetLastError(), "validation kernel");
+        }
+        DevCounters h;
+        if ((rc = read_counters(c, &h))) return rc;
+        if (h.error & kErrCapacity) return fail(c, PARW2V_ERR_ARG, "corpus holds ids outside [0, vocab_size)");
+        c->n_lines = h.n_lines;
+        c->corpus_checked = true;
+        CK(c, cudaMemsetAsync(c->d_cnt, 0, sizeof(DevCounters), c->stream), "counters");
     }
-    DevCounters h;
-    if ((rc = read_counters(c, &h))) return rc;
-    if (h.error & kErrCapacity) return fail(c, PARW2V_ERR_ARG, "corpus holds ids outside [0, vocab_size)");
-    c->n_lines = h.n_lines;
-    TrainArgs a{};
+    TrainArgs a;
+    memset(&a, 0, sizeof(a));  // padding too: the arguments are compared bytewise to reuse graphs
     a.corpus = c->d_corpus;
     a.n_tokens = c->n_tokens;
     a.keep_thr = c->d_thr;
@@ -699,9 +859,8 @@ int parw2v_train(parw2v_ctx *c, parw2v_stats *st) {
     a.packed = c->d_packed;
     a.line_end = c->d_line_end;
     a.max_resample = 1LL << 20;
-    {
-        a.sync_window = c->cfg.attraction == PARW2V_ATTRACT_WINDOW;
-    }
+    a.sync_window = c->cfg.attraction == PARW2V_ATTRACT_WINDOW;
+    a.stage_bulk = c->cfg.staging != PARW2V_STAGING_CPASYNC;
     if (c->cfg.mode == PARW2V_MODE_DET) return train_det(c, a, st);
     rc = ensure_packing(c);
     if (rc) return rc;

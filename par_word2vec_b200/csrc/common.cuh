@@ -16,6 +16,7 @@ constexpr float kExpResolution = 1000.0f / 12.0f;
 // Error bits raised by kernels into the context's device status word.
 constexpr unsigned kErrResample = 1u;  // a negative-resampling loop hit its draw limit
 constexpr unsigned kErrCapacity = 2u;  // an input exceeded a kernel's fixed capacity
+constexpr unsigned kErrStaging = 4u;   // a bulk copy into shared memory did not complete in time
 
 // The reference's linear congruential generator, next = next * 25214903917 + 11 (mod 2^64),
 // PAR_Word2Vec_cpu.cpp:461, :532, :591-612.

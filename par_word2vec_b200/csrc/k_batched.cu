@@ -26,9 +26,12 @@
 // step size and diverges; overwriting loses colliding updates, as the reference's unsynchronised
 // `+=` does.  In BF16 mode the global tables are BF16, working copies and accumulation are FP32,
 // and every write-back rounds stochastically (per-lane LCG bits, the sm_100a cvt.rs conversion).
+#include <algorithm>
+
 #include "common.cuh"
 #include "internal.h"
 #include "mma.cuh"
+#include "repel.cuh"
 #include "sentence.cuh"
 
 namespace parw2v {
@@ -40,35 +43,16 @@ constexpr int kRing = kPrefetch + 1;          // landing buffers for targets / B
 constexpr int kMaxWarpsB = 16;
 constexpr size_t kSmemBudget = 227 * 1024;
 
-// Tensor-core repulsion (BF16 mode): shapes and staging geometry
-constexpr int kMmaK = 48;        // negatives per batch handled by the mma path (3 m-tiles)
-constexpr int kMmaR = 32;        // batch rows handled by the mma path (2 m-tiles / 4 n-tiles)
-// The column chunk is narrow on purpose: shared memory and L1 are one 256 KB array per SM, and
-// every byte of staging taken from it is a byte of L1 the streamed kernel's row reuse loses.
-constexpr int kMmaCols = 32;     // column chunk of the staging
-constexpr int kMmaStride = 40;   // staged row stride in bf16 (80 B: conflict-free ldmatrix rows)
-constexpr int kGbStride = 40;    // bf16 G row stride (80 B)
 __host__ __device__ constexpr size_t up16_c(size_t x) { return (x + 15) & ~(size_t) 15; }
-// FP32 tables on the tensor cores (3xTF32): the same staging bytes hold 16 FP32 columns
-constexpr int kF32Cols = 16;     // column chunk of the FP32 staging
-constexpr int kF32Stride = 20;   // staged FP32 row stride in floats (80 B: conflict-free ldmatrix rows)
-constexpr int kGps = 36;         // FP32 G row stride in floats (144 B: conflict-free ldmatrix rows)
-static_assert(kF32Stride * 4 == kMmaStride * 2, "FP32 and BF16 staging rows take the same bytes");
-
-__host__ __device__ inline bool mma_path(int kmax_eff, int batch) { return kmax_eff <= kMmaK && batch <= kMmaR; }
-__host__ __device__ inline size_t mma_g_bytes(bool bf16) {  // G kept through pass 2
-    return bf16 ? up16_c((size_t) kMmaK * kGbStride * 2) : up16_c((size_t) kMmaK * kGps * 4);
-}
 
 struct Layout {  // per-warp shared-memory carve-up, in bytes (all offsets 16-byte aligned)
     int ws;            // window slots 2w+1+P
-    int ch;            // repulsion column chunk (multiple of 4), SIMT path
+    int ch;            // repulsion column chunk (multiple of 4), CUDA-core path
     int kmax;          // 2 * window * negative
-    bool mma;          // tensor-core repulsion
-    size_t region;     // window cur rows (+ BF16 landing ring) | repulsion staging
+    rep::Geom geo;     // tensor-core repulsion (geo.mma), inside the region
+    size_t region;     // window cur rows (+ BF16 landing ring) | repulsion buffers
     size_t raw_off;    // BF16 landing ring inside the region
-    size_t gb_off;     // mma path: bf16 G inside the region, after the staged chunk
-    size_t tgt_off, g_off, neg_off, dup_off, meta_off, ctx_off, exit_off, per_warp;
+    size_t tgt_off, g_off, neg_off, dup_off, meta_off, ctx_off, exit_off, bar_off, per_warp;
 };
 
 __host__ __device__ inline size_t up16(size_t x) { return (x + 15) & ~(size_t) 15; }
@@ -89,31 +73,26 @@ __host__ __device__ inline Layout make_layout(int ld, int window, int negative, 
     const size_t window_bytes = up16((size_t) L.ws * row32);
     L.raw_off = window_bytes;
     const size_t win_total = window_bytes + (bf16 ? up16((size_t) kRing * row_st) : 0);
-    // the column chunk: as wide as fits in the window's bytes, at least 16 columns
+    // the CUDA-core path's column chunk: as wide as fits in the window's bytes, at least 16 columns
     const size_t rows_rep = (size_t) (batch + L.kmax);
     long ch = (long) (win_total / (rows_rep * 4)) - 4;
     ch = ch / 4 * 4;
     if (ch > ((ld + 3) / 4) * 4) ch = ((ld + 3) / 4) * 4;
     if (ch < 16) ch = 16;
     L.ch = (int) ch;
-    L.mma = mma_path((2 * window - 1) * negative, batch);
-    size_t rep_bytes = up16(rows_rep * (size_t) (L.ch + 4) * 4);
-    L.gb_off = 0;
-    if (L.mma) {
-        const size_t stage = up16((size_t) (kMmaR + kMmaK) * kMmaStride * 2);
-        L.gb_off = stage;
-        rep_bytes = stage + mma_g_bytes(bf16);
-    }
+    L.geo = rep::make_geom(window, negative, batch, bf16);
+    const size_t rep_bytes = L.geo.mma ? L.geo.bytes : up16(rows_rep * (size_t) (L.ch + 4) * 4);
     L.region = win_total > rep_bytes ? win_total : rep_bytes;
     L.tgt_off = L.region;
     L.g_off = L.tgt_off + up16((size_t) kRing * row_st);
-    const size_t g_floats = L.mma ? (size_t) kMmaK * kMmaR : (size_t) L.kmax * batch;
+    const size_t g_floats = L.geo.mma ? 0 : (size_t) L.kmax * batch;
     L.neg_off = L.g_off + up16(g_floats * 4);
     L.dup_off = L.neg_off + up16((size_t) L.kmax * 4);
     L.meta_off = L.dup_off + up16((size_t) (L.kmax + 2 * batch) * 4);
     L.ctx_off = L.meta_off + up16((size_t) L.ws * 8);
     L.exit_off = L.ctx_off + up16((size_t) (2 * window) * 8);
-    L.per_warp = L.exit_off + up16((size_t) kPrefetch * 4 + 16);
+    L.bar_off = L.exit_off + up16((size_t) kPrefetch * 4 + 16);
+    L.per_warp = L.bar_off + 16;
     return L;
 }
 
@@ -198,456 +177,6 @@ struct Store<true> {  // BF16 tables
 };
 
 
-// Repeated words of a batch: dup[k] (negatives) and dup[K + r] (batch rows) get the index of the
-// word's first occurrence, or -1.  Generic form (any K, rows).
-__device__ __noinline__ void mark_repeats(const int *negs, int K, const int32_t *batch_words, int rows, int *dup,
-                                          int lane) {
-    for (int k = lane; k < K; k += 32) {
-        int first = -1;
-        for (int q = 0; q < k && first < 0; q++)
-            if (negs[q] == negs[k]) first = q;
-        dup[k] = first;
-    }
-    for (int r = lane; r < rows; r += 32) {
-        int first = -1;
-        const int wr = __ldg(batch_words + r);
-        for (int q = 0; q < r && first < 0; q++)
-            if (__ldg(batch_words + q) == wr) first = q;
-        dup[K + r] = first;
-    }
-    __syncwarp();
-}
-
-// The same marks for K <= 64 negatives and rows <= 32 (the tensor-core paths), by warp matching:
-// lanes holding equal words find each other in one __match_any_sync; negatives 32..63 also look
-// through the first 32 by shuffles.  Lanes without a word hold distinct negative sentinels.
-__device__ __forceinline__ void mark_repeats_small(const int *negs, int K, const int *words, int rows, int *dup,
-                                                   int lane) {
-    const int wr = lane < rows ? words[lane] : -1 - lane;
-    const unsigned mr = __match_any_sync(0xffffffffu, wr);
-    if (lane < rows) dup[K + lane] = (__ffs(mr) - 1 == lane) ? -1 : __ffs(mr) - 1;
-    const int v0 = lane < K ? negs[lane] : -1 - lane;
-    const unsigned m0 = __match_any_sync(0xffffffffu, v0);
-    if (lane < K) dup[lane] = (__ffs(m0) - 1 == lane) ? -1 : __ffs(m0) - 1;
-    if (K > 32) {
-        const int v1 = lane + 32 < K ? negs[lane + 32] : -100 - lane;
-        int first = -1;
-        for (int q = 0; q < 32; q++) {
-            const int w = __shfl_sync(0xffffffffu, v0, q);
-            if (first < 0 && q < K && w == v1) first = q;
-        }
-        const unsigned m1 = __match_any_sync(0xffffffffu, v1);
-        if (first < 0 && __ffs(m1) - 1 != lane) first = 32 + __ffs(m1) - 1;
-        if (lane + 32 < K) dup[lane + 32] = first;
-    }
-    __syncwarp();
-}
-
-// Merge the gradient columns of repeated batch rows, then the gradient rows of repeated negatives,
-// into their first occurrence (G is K x rows with row stride gs), so each distinct row is written
-// once.  Only the marked rows are visited, in ascending order (32 at a time by ballot).
-__device__ __noinline__ void merge_marked(int K, int rows, float *G, int gs, const int *dup, int lane) {
-    for (int r0 = 0; r0 < rows; r0 += 32) {
-        for (unsigned m = __ballot_sync(0xffffffffu, r0 + lane < rows && dup[K + r0 + lane] >= 0); m; m &= m - 1) {
-            const int r = r0 + __ffs(m) - 1, f = dup[K + r];
-            for (int k = lane; k < K; k += 32) {
-                G[k * gs + f] += G[k * gs + r];
-                G[k * gs + r] = 0.f;
-            }
-            __syncwarp();
-        }
-    }
-    for (int k0 = 0; k0 < K; k0 += 32) {
-        for (unsigned m = __ballot_sync(0xffffffffu, k0 + lane < K && dup[k0 + lane] >= 0); m; m &= m - 1) {
-            const int k = k0 + __ffs(m) - 1, f = dup[k];
-            for (int r = lane; r < rows; r += 32) {
-                G[f * gs + r] += G[k * gs + r];
-                G[k * gs + r] = 0.f;
-            }
-            __syncwarp();
-        }
-    }
-}
-
-__device__ __forceinline__ void merge_repeats(const int *negs, int K, const int32_t *batch_words, int rows, float *G,
-                                              int gs, int *dup, int lane) {
-    mark_repeats(negs, K, batch_words, rows, dup, lane);
-    merge_marked(K, rows, G, gs, dup, lane);
-}
-
-// Repulsion of one batch on the tensor cores (BF16 tables, K <= 48 negatives, rows <= 32).
-// Column chunks of M_in (rows) and M_out (negatives) are staged as BF16 with cp.async.
-// Pass 1 accumulates G = M_out M_in^T over all chunks in registers (m16n8k16, FP32 accumulate);
-// G = alpha * (0 - sigma(G)) through the table, repeated words merged, G rounded to BF16.
-// Pass 2 re-stages each chunk, forms M_out + G M_in and M_in + G^T M_out 8 columns at a time,
-// rounds them stochastically into the staged tile in place and stores every distinct row's
-// 16-byte pieces back to the tables.
-__device__ __noinline__ void repel_mma(const TrainArgs &a, const Layout &Lo, unsigned char *base, const int32_t *bw,
-                                       int rows, const int *negs, int K, float alpha, const float *s_exp, float *Gf,
-                                       int *dup, int lane, LaneBits &rb) {
-    using T = __nv_bfloat16;
-    T *w_in = static_cast<T *>(a.w_in);
-    T *w_out = static_cast<T *>(a.w_out);
-    const int ld = a.ld;
-    T *sin = reinterpret_cast<T *>(base);                        // kMmaR x kMmaStride
-    T *sout = sin + (size_t) kMmaR * kMmaStride;                  // kMmaK x kMmaStride
-    T *Gb = reinterpret_cast<T *>(base + Lo.gb_off);              // kMmaK x kGbStride
-    const int g = lane >> 2, t = lane & 3;
-    const int mt1 = (K + 15) >> 4;        // m-tiles of negatives
-    const int nt1 = (rows + 7) >> 3;      // n-tiles of batch rows (pass 1)
-    const int kr = (rows + 15) >> 4;      // 16-row steps of the batch (pass 2)
-    constexpr int kPieces = kMmaCols / 8; // 16-byte pieces per staged row
-    float acc[3][4][4];
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-#pragma unroll
-            for (int e = 0; e < 4; e++) acc[i][j][e] = 0.f;
-    // the batch's words, read once: the staging and write-back loops index them per piece
-    int *sbw = dup + Lo.kmax + a.batch;
-    if (lane < rows) sbw[lane] = __ldg(bw + lane);
-    __syncwarp();
-#pragma unroll 1
-    for (int pass = 0; pass < 2; pass++) {
-        // zero the padding rows the products read (batch rows up to kMmaR, negatives up to the
-        // m-tile), columns 0..kMmaCols-1; they stay zero for every chunk of the pass, since the
-        // staging writes only the real rows (the FP32 G of pass 1 may share these bytes, see the
-        // streamed kernel, so pass 2 zeroes them again)
-        const int pad_in = kMmaR - rows, pad_out = 16 * mt1 - K;
-        for (int i = lane; i < (pad_in + pad_out) * kPieces; i += 32) {
-            const int pr = i / kPieces, q = i - pr * kPieces;
-            T *row = pr < pad_in ? sin + (size_t) (rows + pr) * kMmaStride : sout + (size_t) (K + pr - pad_in) * kMmaStride;
-            reinterpret_cast<uint4 *>(row)[q] = make_uint4(0, 0, 0, 0);
-        }
-        __syncwarp();
-#pragma unroll 1
-        for (int col0 = 0; col0 < ld; col0 += kMmaCols) {
-            // stage columns [col0, col0 + kMmaCols) of the batch rows and the negatives' rows
-            for (int it = lane; it < (rows + K) * kPieces; it += 32) {
-                const int rr = it / kPieces, pc = it - rr * kPieces;
-                T *dst = (rr < rows ? sin + (size_t) rr * kMmaStride : sout + (size_t) (rr - rows) * kMmaStride) + pc * 8;
-                const int col = col0 + pc * 8;
-                if (col < ld) {
-                    const T *src = (rr < rows ? w_in + (size_t) sbw[rr] * ld : w_out + (size_t) negs[rr - rows] * ld) + col;
-                    cp_async16(dst, src);
-                } else {
-                    *reinterpret_cast<uint4 *>(dst) = make_uint4(0, 0, 0, 0);
-                }
-            }
-            cp_async_commit();
-            cp_async_wait_all();
-            __syncwarp();
-            if (pass == 0) {
-#pragma unroll 1
-                for (int ks = 0; ks < kMmaCols / 16; ks++) {
-                    unsigned bfr[4][2];
-#pragma unroll
-                    for (int np = 0; np < 2; np++) {  // n-tiles 2np, 2np+1 in one ldmatrix.x4
-                        unsigned r[4];
-                        const int n = np * 16 + (lane & 7) + ((lane >> 4) << 3);
-                        ldsm_x4(r, sin + (size_t) n * kMmaStride + ks * 16 + ((lane >> 3) & 1) * 8);
-                        bfr[2 * np][0] = r[0];
-                        bfr[2 * np][1] = r[1];
-                        bfr[2 * np + 1][0] = r[2];
-                        bfr[2 * np + 1][1] = r[3];
-                    }
-#pragma unroll
-                    for (int mt = 0; mt < 3; mt++)
-                        if (mt < mt1) {
-                            unsigned af[4];
-                            ldsm_x4(af, sout + (size_t) (mt * 16 + (lane & 15)) * kMmaStride + ks * 16 + (lane >> 4) * 8);
-#pragma unroll
-                            for (int nt = 0; nt < 4; nt++)
-                                if (nt < nt1) mma16816(acc[mt][nt], af, bfr[nt][0], bfr[nt][1]);
-                        }
-                }
-            } else {
-                const int ncols = min(kMmaCols, ld - col0);
-#pragma unroll 1
-                for (int nt = 0; nt < ncols / 8; nt++) {
-                    float o[3][4], q[2][4];
-#pragma unroll
-                    for (int e = 0; e < 4; e++) {
-                        o[0][e] = o[1][e] = o[2][e] = 0.f;
-                        q[0][e] = q[1][e] = 0.f;
-                    }
-                    // M_out update: G (K x rows) . M_in (rows x 8 columns)
-#pragma unroll 1
-                    for (int ks = 0; ks < kr; ks++) {
-                        unsigned b[2];
-                        ldsm_x2_t(b, sin + (size_t) (ks * 16 + (lane & 15)) * kMmaStride + nt * 8);
-#pragma unroll
-                        for (int mt = 0; mt < 3; mt++)
-                            if (mt < mt1) {
-                                unsigned af[4];
-                                ldsm_x4(af, Gb + (size_t) (mt * 16 + (lane & 15)) * kGbStride + ks * 16 + (lane >> 4) * 8);
-                                mma16816(o[mt], af, b[0], b[1]);
-                            }
-                    }
-                    // M_in update: G^T (rows x K) . M_out (K x 8 columns)
-#pragma unroll 1
-                    for (int ks = 0; ks < mt1; ks++) {
-                        unsigned b[2];
-                        ldsm_x2_t(b, sout + (size_t) (ks * 16 + (lane & 15)) * kMmaStride + nt * 8);
-#pragma unroll
-                        for (int mt = 0; mt < 2; mt++)
-                            if (mt < kr) {
-                                unsigned af[4];
-                                ldsm_x4_t(af, Gb + (size_t) (ks * 16 + ((lane >> 4) << 3) + (lane & 7)) * kGbStride +
-                                                  mt * 16 + ((lane >> 3) & 1) * 8);
-                                mma16816(q[mt], af, b[0], b[1]);
-                            }
-                    }
-                    // new values = staged + update, rounded stochastically, in place
-                    const int j = nt * 8 + 2 * t;
-#pragma unroll
-                    for (int mt = 0; mt < 3; mt++)
-                        if (mt < mt1) {
-                            const uint64_t bits = rb.next();
-#pragma unroll
-                            for (int h = 0; h < 2; h++) {
-                                __nv_bfloat162 *cell = reinterpret_cast<__nv_bfloat162 *>(sout + (size_t) (mt * 16 + g + 8 * h) * kMmaStride + j);
-                                const float2 old = __bfloat1622float2(*cell);
-                                *reinterpret_cast<unsigned *>(cell) =
-                                    pack_sr2(make_float2(old.x + o[mt][2 * h], old.y + o[mt][2 * h + 1]), bits >> (32 * h));
-                            }
-                        }
-#pragma unroll
-                    for (int mt = 0; mt < 2; mt++)
-                        if (mt < kr) {
-                            const uint64_t bits = rb.next();
-#pragma unroll
-                            for (int h = 0; h < 2; h++) {
-                                __nv_bfloat162 *cell = reinterpret_cast<__nv_bfloat162 *>(sin + (size_t) (mt * 16 + g + 8 * h) * kMmaStride + j);
-                                const float2 old = __bfloat1622float2(*cell);
-                                *reinterpret_cast<unsigned *>(cell) =
-                                    pack_sr2(make_float2(old.x + q[mt][2 * h], old.y + q[mt][2 * h + 1]), bits >> (32 * h));
-                            }
-                        }
-                }
-                __syncwarp();
-                // each distinct row's new chunk back to its table in 16-byte pieces
-                for (int it = lane; it < (rows + K) * kPieces; it += 32) {
-                    const int rr = it / kPieces, pc = it - rr * kPieces;
-                    const int col = col0 + pc * 8;
-                    if (col >= ld || dup[rr < rows ? K + rr : rr - rows] >= 0) continue;
-                    const T *src = (rr < rows ? sin + (size_t) rr * kMmaStride : sout + (size_t) (rr - rows) * kMmaStride) + pc * 8;
-                    T *dst = (rr < rows ? w_in + (size_t) sbw[rr] * ld : w_out + (size_t) negs[rr - rows] * ld) + col;
-                    *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(src);
-                }
-            }
-            __syncwarp();
-        }
-        if (pass == 0) {
-            // raw dot products into Gf (kMmaK x kMmaR), sigma / label 0, merge repeats, BF16 copy
-#pragma unroll
-            for (int mt = 0; mt < 3; mt++)
-#pragma unroll
-                for (int nt = 0; nt < 4; nt++)
-#pragma unroll
-                    for (int e = 0; e < 4; e++)
-                        if (mt < mt1 && nt < nt1) {
-                            const int k = mt * 16 + g + ((e >> 1) << 3), r = nt * 8 + 2 * t + (e & 1);
-                            if (k < K && r < rows) Gf[k * kMmaR + r] = grad_from_table(acc[mt][nt][e], 0, alpha, s_exp);
-                        }
-            mark_repeats_small(negs, K, sbw, rows, dup, lane);
-            merge_marked(K, rows, Gf, kMmaR, dup, lane);
-            // BF16 G over the part pass 2 reads: negatives below 16 * mt1, batch rows below 16 * kr
-            const int sh = kr == 1 ? 3 : 4;  // column pairs per row: 8 * kr
-            for (int i = lane; i < (16 * mt1) << sh; i += 32) {
-                const int k = i >> sh, r = 2 * (i & ((1 << sh) - 1));
-                const float v0 = (k < K && r < rows) ? Gf[k * kMmaR + r] : 0.f;
-                const float v1 = (k < K && r + 1 < rows) ? Gf[k * kMmaR + r + 1] : 0.f;
-                reinterpret_cast<__nv_bfloat162 *>(Gb + (size_t) k * kGbStride)[r >> 1] = __floats2bfloat162_rn(v0, v1);
-            }
-            __syncwarp();
-        }
-    }
-}
-
-// Repulsion of one batch on the tensor cores with FP32 tables (K <= 48 negatives, rows <= 32): the
-// structure of repel_mma with FP32 staging (16-column chunks) and 3xTF32 products, so the FP32 mode
-// keeps FP32-level arithmetic.  G stays FP32 through pass 2 (kMmaK x kGps floats), and the new
-// values (staged value + update) go from the accumulators straight to the rows.
-__device__ __noinline__ void repel_mma_f32(const TrainArgs &a, const Layout &Lo, unsigned char *base, const int32_t *bw,
-                                           int rows, const int *negs, int K, float alpha, const float *s_exp, float *Gf,
-                                           int *dup, int lane) {
-    float *w_in = static_cast<float *>(a.w_in);
-    float *w_out = static_cast<float *>(a.w_out);
-    const int ld = a.ld;
-    float *sin = reinterpret_cast<float *>(base);             // kMmaR x kF32Stride
-    float *sout = sin + (size_t) kMmaR * kF32Stride;          // kMmaK x kF32Stride
-    float *Gp = reinterpret_cast<float *>(base + Lo.gb_off);  // kMmaK x kGps
-    const int g = lane >> 2, t = lane & 3;
-    const int mt1 = (K + 15) >> 4;  // m-tiles of negatives
-    const int nt1 = (rows + 7) >> 3;  // n-tiles of batch rows (pass 1)
-    const int kr8 = (rows + 7) >> 3;  // 8-row k-steps over the batch rows
-    const int kk8 = (K + 7) >> 3;     // 8-row k-steps over the negatives
-    const int mr = (rows + 15) >> 4;  // m-tiles of batch rows (pass 2)
-    constexpr int kPieces = kF32Cols / 4;  // 16-byte pieces per staged row
-    float acc[3][4][4];
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-#pragma unroll
-            for (int e = 0; e < 4; e++) acc[i][j][e] = 0.f;
-    // the batch's words, read once: the staging and write-back loops index them per piece
-    int *sbw = dup + Lo.kmax + a.batch;
-    if (lane < rows) sbw[lane] = __ldg(bw + lane);
-    __syncwarp();
-#pragma unroll 1
-    for (int pass = 0; pass < 2; pass++) {
-        // zero the staging: padding rows stay zero for every chunk of the pass
-        for (int i = lane; i < (kMmaR + kMmaK) * kF32Stride / 4; i += 32)
-            reinterpret_cast<float4 *>(sin)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        __syncwarp();
-#pragma unroll 1
-        for (int col0 = 0; col0 < ld; col0 += kF32Cols) {
-            for (int it = lane; it < (rows + K) * kPieces; it += 32) {
-                const int rr = it / kPieces, pc = it - rr * kPieces;
-                float *dst = (rr < rows ? sin + (size_t) rr * kF32Stride : sout + (size_t) (rr - rows) * kF32Stride) + pc * 4;
-                const int col = col0 + pc * 4;
-                if (col < ld) {
-                    const float *src = (rr < rows ? w_in + (size_t) sbw[rr] * ld : w_out + (size_t) negs[rr - rows] * ld) + col;
-                    cp_async16(dst, src);
-                } else {
-                    *reinterpret_cast<float4 *>(dst) = make_float4(0.f, 0.f, 0.f, 0.f);
-                }
-            }
-            cp_async_commit();
-            cp_async_wait_all();
-            __syncwarp();
-            if (pass == 0) {
-                // S += M_out . M_in^T over these 16 columns: two k-steps of 8
-#pragma unroll 1
-                for (int ks = 0; ks < kF32Cols / 8; ks++) {
-                    unsigned bb[4][2], bs[4][2];
-#pragma unroll
-                    for (int np = 0; np < 2; np++) {  // n-tiles 2np, 2np+1 in one ldmatrix.x4
-                        float r[4];
-                        const int n = np * 16 + (lane & 7) + ((lane >> 4) << 3);
-                        ldsm_x4_f32(r, sin + (size_t) n * kF32Stride + ks * 8 + ((lane >> 3) & 1) * 4);
-#pragma unroll
-                        for (int h = 0; h < 2; h++) {
-                            split_tf32(r[2 * h], bb[2 * np + h][0], bs[2 * np + h][0]);
-                            split_tf32(r[2 * h + 1], bb[2 * np + h][1], bs[2 * np + h][1]);
-                        }
-                    }
-#pragma unroll
-                    for (int mt = 0; mt < 3; mt++)
-                        if (mt < mt1) {
-                            float af[4];
-                            ldsm_x4_f32(af, sout + (size_t) (mt * 16 + (lane & 7) + ((lane >> 3) & 1) * 8) * kF32Stride + ks * 8 +
-                                                (lane >> 4) * 4);
-                            unsigned ab[4], as[4];
-                            split_a(af, ab, as);
-#pragma unroll
-                            for (int nt = 0; nt < 4; nt++)
-                                if (nt < nt1) mma3xtf32(acc[mt][nt], ab, as, bb[nt], bs[nt]);
-                        }
-                }
-            } else {
-#pragma unroll 1
-                for (int nt = 0; nt < kF32Cols / 8; nt++) {
-                    const int cb = nt * 8;
-                    if (col0 + cb >= ld) break;
-                    float o[3][4], q[2][4];
-#pragma unroll
-                    for (int e = 0; e < 4; e++) {
-                        o[0][e] = o[1][e] = o[2][e] = 0.f;
-                        q[0][e] = q[1][e] = 0.f;
-                    }
-                    // M_out update: G (K x rows) . M_in (rows x 8 columns)
-#pragma unroll 1
-                    for (int ks = 0; ks < kr8; ks++) {
-                        unsigned bb[2], bs[2];
-                        split_tf32(sin[(size_t) (ks * 8 + t) * kF32Stride + cb + g], bb[0], bs[0]);
-                        split_tf32(sin[(size_t) (ks * 8 + t + 4) * kF32Stride + cb + g], bb[1], bs[1]);
-#pragma unroll
-                        for (int mt = 0; mt < 3; mt++)
-                            if (mt < mt1) {
-                                float af[4];
-                                ldsm_x4_f32(af, Gp + (size_t) (mt * 16 + (lane & 7) + ((lane >> 3) & 1) * 8) * kGps + ks * 8 +
-                                                    (lane >> 4) * 4);
-                                unsigned ab[4], as[4];
-                                split_a(af, ab, as);
-                                mma3xtf32(o[mt], ab, as, bb, bs);
-                            }
-                    }
-                    // M_in update: G^T (rows x K) . M_out (K x 8 columns)
-#pragma unroll 1
-                    for (int ks = 0; ks < kk8; ks++) {
-                        unsigned bb[2], bs[2];
-                        split_tf32(sout[(size_t) (ks * 8 + t) * kF32Stride + cb + g], bb[0], bs[0]);
-                        split_tf32(sout[(size_t) (ks * 8 + t + 4) * kF32Stride + cb + g], bb[1], bs[1]);
-#pragma unroll
-                        for (int mt = 0; mt < 2; mt++)
-                            if (mt < mr) {
-                                const float *gk = Gp + (size_t) (ks * 8 + t) * kGps + mt * 16 + g;
-                                const float af[4] = {gk[0], gk[8], gk[4 * kGps], gk[4 * kGps + 8]};
-                                unsigned ab[4], as[4];
-                                split_a(af, ab, as);
-                                mma3xtf32(q[mt], ab, as, bb, bs);
-                            }
-                    }
-                    // staged value + update, straight to the rows (each distinct word once)
-                    const int c = cb + 2 * t;
-                    if (col0 + c < ld) {
-#pragma unroll
-                        for (int mt = 0; mt < 3; mt++)
-                            if (mt < mt1)
-#pragma unroll
-                                for (int h = 0; h < 2; h++) {
-                                    const int row = mt * 16 + g + 8 * h;
-                                    if (row < K && dup[row] < 0) {
-                                        const float2 old = *reinterpret_cast<const float2 *>(sout + (size_t) row * kF32Stride + c);
-                                        *reinterpret_cast<float2 *>(w_out + (size_t) negs[row] * ld + col0 + c) =
-                                            make_float2(old.x + o[mt][2 * h], old.y + o[mt][2 * h + 1]);
-                                    }
-                                }
-#pragma unroll
-                        for (int mt = 0; mt < 2; mt++)
-                            if (mt < mr)
-#pragma unroll
-                                for (int h = 0; h < 2; h++) {
-                                    const int row = mt * 16 + g + 8 * h;
-                                    if (row < rows && dup[K + row] < 0) {
-                                        const float2 old = *reinterpret_cast<const float2 *>(sin + (size_t) row * kF32Stride + c);
-                                        *reinterpret_cast<float2 *>(w_in + (size_t) sbw[row] * ld + col0 + c) =
-                                            make_float2(old.x + q[mt][2 * h], old.y + q[mt][2 * h + 1]);
-                                    }
-                                }
-                    }
-                }
-            }
-            __syncwarp();
-        }
-        if (pass == 0) {
-            // raw dot products into Gf (kMmaK x kMmaR), sigma / label 0, merge repeats, then the FP32
-            // copy that pass 2 reads (zero outside K x rows)
-#pragma unroll
-            for (int mt = 0; mt < 3; mt++)
-#pragma unroll
-                for (int nt = 0; nt < 4; nt++)
-#pragma unroll
-                    for (int e = 0; e < 4; e++)
-                        if (mt < mt1 && nt < nt1) {
-                            const int k = mt * 16 + g + ((e >> 1) << 3), r = nt * 8 + 2 * t + (e & 1);
-                            if (k < K && r < rows) Gf[k * kMmaR + r] = grad_from_table(acc[mt][nt][e], 0, alpha, s_exp);
-                        }
-            mark_repeats_small(negs, K, sbw, rows, dup, lane);
-            merge_marked(K, rows, Gf, kMmaR, dup, lane);
-            for (int i = lane; i < kMmaK * kMmaR; i += 32) {
-                const int k = i / kMmaR, r = i - k * kMmaR;
-                Gp[(size_t) k * kGps + r] = (k < K && r < rows) ? Gf[i] : 0.f;
-            }
-            __syncwarp();
-        }
-    }
-}
-
 // Repulsion of one batch on the CUDA cores (FP32 tables, or shapes beyond the mma path): G is
 // accumulated over column chunks staged as FP32, then a second pass writes the new rows.
 template <bool BF16>
@@ -692,7 +221,8 @@ __device__ __noinline__ void repel_simt(const TrainArgs &a, const Layout &Lo, un
     }
     for (int e = lane; e < K * rows; e += 32) G[e] = grad_from_table(G[e], 0, alpha, s_exp);
     __syncwarp();
-    merge_repeats(negs, K, bw, rows, G, rows, dup, lane);
+    rep::mark_repeats(negs, K, bw, rows, dup, lane);
+    rep::merge_marked(K, rows, G, rows, dup, lane);
     for (int col0 = 0; col0 < ld; col0 += Lo.ch) {
         stage_chunk(col0);
         const int ncol4 = min(c4, (ld - col0 + 3) / 4);
@@ -725,6 +255,35 @@ __device__ __noinline__ void repel_simt(const TrainArgs &a, const Layout &Lo, un
     }
 }
 
+// The repulsion of one batch on the path its shapes allow (tensor cores for rows <= 32 and at most
+// 96 negatives, else CUDA cores).  False if the staging could not complete: the caller stops.
+template <bool BF16>
+__device__ __forceinline__ bool repel_batch(const TrainArgs &a, const Layout &Lo, unsigned char *base, const int32_t *bw,
+                                            int rows, const int *negs, int K, float alpha, const float *s_exp, float *G,
+                                            int *dup, int lane, LaneBits &rb, rep::Stager &st) {
+    if (Lo.geo.mma) {
+        int *sbw = dup + Lo.kmax + a.batch;  // the batch's words, read once
+        if (lane < rows) sbw[lane] = __ldg(bw + lane);
+        __syncwarp();
+        if constexpr (BF16) {
+            return rep::repel_bf16(a, Lo.geo, base, sbw, rows, negs, K, alpha, s_exp, dup, lane, rb, st);
+        } else {
+            return Lo.geo.mt <= 3 ? rep::repel_f32<3>(a, Lo.geo, base, sbw, rows, negs, K, alpha, s_exp, dup, lane, st)
+                                  : rep::repel_f32<6>(a, Lo.geo, base, sbw, rows, negs, K, alpha, s_exp, dup, lane, st);
+        }
+    }
+    repel_simt<BF16>(a, Lo, base, bw, rows, negs, K, alpha, s_exp, G, dup, lane, rb);
+    return true;
+}
+
+// The warp's staging barrier, initialised once per warp before any copy uses it.
+__device__ __forceinline__ rep::Stager make_stager(unsigned char *bar_mem, int stage_bulk, int lane) {
+    uint64_t *bar = reinterpret_cast<uint64_t *>(bar_mem);
+    if (lane == 0) mbar_init(bar, 1);
+    __syncwarp();
+    return rep::Stager{bar, 0u, stage_bulk != 0};
+}
+
 template <int NV4, bool BF16, bool SYNC>
 __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs a, int warps) {
     using S = Store<BF16>;
@@ -752,18 +311,19 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
     float *ctx_g = reinterpret_cast<float *>(base + Lo.ctx_off);        // 2w: window-synchronous gradients
     int *ctx_s = reinterpret_cast<int *>(ctx_g + 2 * w);                 // 2w: and context slots
     int *recent_exit = reinterpret_cast<int *>(base + Lo.exit_off);      // words written back lately
+    rep::Stager st = make_stager(base + Lo.bar_off, a.stage_bulk, lane);
 
     T *w_in = static_cast<T *>(a.w_in);
     T *w_out = static_cast<T *>(a.w_out);
     const uint64_t n_lines = a.cnt->n_lines, total_kept = a.cnt->total_kept;
     const int epoch = hogwild_epoch(a);
     const int row_chunks = ld / S::kChunkElems;  // 16-byte pieces per stored row
-    const bool use_mma = Lo.mma;
     // c mod ws for positions c < 2^16 by a multiply-high reciprocal (exact: ws <= 256)
     const unsigned ws_u = (unsigned) Lo.ws, ws_m = (unsigned) (0xFFFFFFFFULL / ws_u) + 1u;
     auto ring = [&](int c) { return (int) ((unsigned) c - __umulhi((unsigned) c, ws_m) * ws_u); };
     unsigned long long st_kept = 0, st_sent = 0, st_pairs = 0, st_batches = 0, st_negs = 0;
     bool failed = false;
+    unsigned fail_bits = 0;
 
     for (;;) {
         unsigned long long line = 0;
@@ -1002,22 +562,15 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
                 const int K = rep_b * a.negative;
                 if (!warp_draw_negatives(a.table, a.vocab, rng, sen, L, K, negs, lane, a.max_resample)) {
                     failed = true;  // unresolved negatives: leave the batch untouched
+                    fail_bits |= kErrResample;
                     break;
                 }
                 st_batches++;
                 st_negs += K;
-                if (K > 0) {
-                    if constexpr (BF16) {
-                        if (use_mma)
-                            repel_mma(a, Lo, base, sen + lo_b, rows, negs, K, alpha, s_exp, G, dup, lane, rb);
-                        else
-                            repel_simt<true>(a, Lo, base, sen + lo_b, rows, negs, K, alpha, s_exp, G, dup, lane, rb);
-                    } else {
-                        if (use_mma)
-                            repel_mma_f32(a, Lo, base, sen + lo_b, rows, negs, K, alpha, s_exp, G, dup, lane);
-                        else
-                            repel_simt<false>(a, Lo, base, sen + lo_b, rows, negs, K, alpha, s_exp, G, dup, lane, rb);
-                    }
+                if (K > 0 && !repel_batch<BF16>(a, Lo, base, sen + lo_b, rows, negs, K, alpha, s_exp, G, dup, lane, rb, st)) {
+                    failed = true;  // a staging copy did not complete
+                    fail_bits |= kErrStaging;
+                    break;
                 }
                 __threadfence_block();
                 __syncwarp();
@@ -1032,7 +585,7 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
         atomicAdd(&a.cnt->pairs, st_pairs);
         atomicAdd(&a.cnt->batches, st_batches);
         atomicAdd(&a.cnt->negatives, st_negs);
-        if (failed) atomicOr(&a.cnt->error, kErrResample);
+        if (fail_bits) atomicOr(&a.cnt->error, fail_bits);
     }
 }
 
@@ -1060,50 +613,150 @@ cudaError_t launch_nv(const TrainArgs &a, int grid, int warps, cudaStream_t s) {
 // sentences are in flight per SM and more of the unified L1 is left to cache rows.
 constexpr int kMaxWarpsS = 16;
 constexpr int kStreamStats = 5;  // kept, sentences, pairs, batches, negatives (per warp, in shared memory)
-constexpr size_t kStreamStage = (size_t) (kMmaR + kMmaK) * kMmaStride * 2;  // 6,400 bytes
-static_assert(kStreamStage >= (size_t) kMmaK * kMmaR * 4, "the FP32 G of pass 1 shares the staging bytes");
+constexpr size_t kSimtStage = 6400;  // CUDA-core repulsion staging bytes (column chunk as wide as fits)
 
 __host__ __device__ inline Layout make_layout_stream(int ld, int window, int negative, int batch, bool bf16) {
     Layout L;
     L.ws = 0;
     L.kmax = 2 * window * negative;
-    L.mma = mma_path((2 * window - 1) * negative, batch);
+    L.geo = rep::make_geom(window, negative, batch, bf16);
     L.raw_off = 0;
     L.tgt_off = 0;
     L.meta_off = 0;
     const size_t rows_rep = (size_t) (batch + L.kmax);
-    long ch = (long) (kStreamStage / (rows_rep * 4)) - 4;
+    long ch = (long) (kSimtStage / (rows_rep * 4)) - 4;
     ch = ch / 4 * 4;
     if (ch > ((ld + 3) / 4) * 4) ch = ((ld + 3) / 4) * 4;
     if (ch < 16) ch = 16;
     L.ch = (int) ch;
-    if (L.mma) {
-        L.gb_off = kStreamStage;
-        L.region = kStreamStage + mma_g_bytes(bf16);
-        L.g_off = 0;  // the FP32 G of pass 1 shares the staging bytes
+    if (L.geo.mma) {
+        L.region = L.geo.bytes;
+        L.g_off = 0;  // unused: the tensor-core paths keep G inside the region
     } else {
-        L.gb_off = 0;
         L.region = up16(rows_rep * (size_t) (L.ch + 4) * 4);
         L.g_off = L.region;
     }
-    const size_t g_bytes = L.mma ? 0 : up16((size_t) L.kmax * batch * 4);
+    const size_t g_bytes = L.geo.mma ? 0 : up16((size_t) L.kmax * batch * 4);
     L.neg_off = L.region + g_bytes;
     L.dup_off = L.neg_off + up16((size_t) L.kmax * 4);
     L.ctx_off = L.dup_off + up16((size_t) (L.kmax + 2 * batch) * 4);
     L.exit_off = L.ctx_off + up16((size_t) (2 * window) * 8);
-    L.per_warp = L.exit_off + up16(kStreamStats * sizeof(unsigned long long));  // the warp's statistics
+    L.bar_off = L.exit_off + up16(kStreamStats * sizeof(unsigned long long));  // after the warp's statistics
+    L.per_warp = L.bar_off + 16;
     return L;
 }
 
-template <int NV4, bool BF16, bool SYNC>
+// A table row as one warp holds it in the streamed kernel: E elements per lane (d <= 32 E), in up to
+// three chunks of 16, 8 and 4 bytes.  Chunk j of 16 bytes covers elements j * 32 * EA + lane * EA
+// (EA = 8 BF16 / 4 FP32); the 8-byte chunk (EB = 4 / 2 elements) and the 4-byte chunk (EC = 2 / 1)
+// follow them.  At d = 300, BF16, that is one 16-byte and one 4-byte chunk per lane: 10 elements,
+// 320 slots for 300 values (a lane of only 16-byte... chunks would hold 12 or 16).  Chunks that lie
+// beyond the row's ld elements are neither read nor written; elements in [d, ld) are the row's zero
+// padding and stay zero (0 + g * 0).
+template <bool BF16, int E>
+struct LaneRow {
+    using T = typename Store<BF16>::T;
+    static constexpr int EA = BF16 ? 8 : 4, EB = BF16 ? 4 : 2, EC = BF16 ? 2 : 1;
+    static constexpr int NA = E / EA;
+    static constexpr int NB = (E - NA * EA) / EB;
+    static constexpr int NC = (E - NA * EA - NB * EB) / EC;
+    static_assert(NA * EA + NB * EB + NC * EC == E && NB <= 1 && NC <= 1, "E must split into the chunk sizes");
+    static constexpr int W = NA * 4 + NB * 2 + NC;  // 32-bit words per lane as stored
+    static constexpr int OFF_B = NA * 32 * EA, OFF_C = OFF_B + NB * 32 * EB;
+    struct Raw {
+        uint32_t w[W];
+    };
+    // which chunks of this lane lie inside a row of ld elements: bits 0..NA-1, NA (B), NA+1 (C)
+    __device__ static unsigned valid_mask(int lane, int ld) {
+        unsigned m = 0;
+#pragma unroll
+        for (int j = 0; j < NA; j++)
+            if (j * 32 * EA + (lane + 1) * EA <= ld) m |= 1u << j;
+        if (NB && OFF_B + (lane + 1) * EB <= ld) m |= 1u << NA;
+        if (NC && OFF_C + (lane + 1) * EC <= ld) m |= 2u << NA;
+        return m;
+    }
+    // the lane's chunks of a table row, read at L2 (never from this SM's non-coherent L1)
+    __device__ static Raw load(const T *row, int lane, unsigned vm) {
+        Raw r;
+#pragma unroll
+        for (int j = 0; j < NA; j++) {
+            uint4 u = make_uint4(0u, 0u, 0u, 0u);
+            if (vm & (1u << j)) u = __ldcg(reinterpret_cast<const uint4 *>(row + j * 32 * EA) + lane);
+            r.w[4 * j] = u.x;
+            r.w[4 * j + 1] = u.y;
+            r.w[4 * j + 2] = u.z;
+            r.w[4 * j + 3] = u.w;
+        }
+        if (NB) {
+            uint2 u = make_uint2(0u, 0u);
+            if (vm & (1u << NA)) u = __ldcg(reinterpret_cast<const uint2 *>(row + OFF_B) + lane);
+            r.w[4 * NA] = u.x;
+            r.w[4 * NA + 1] = u.y;
+        }
+        if (NC) {
+            unsigned u = 0u;
+            if (vm & (2u << NA)) u = __ldcg(reinterpret_cast<const unsigned *>(row + OFF_C) + lane);
+            r.w[W - 1] = u;
+        }
+        return r;
+    }
+    __device__ static void store(T *row, const Raw &r, int lane, unsigned vm) {
+#pragma unroll
+        for (int j = 0; j < NA; j++)
+            if (vm & (1u << j))
+                reinterpret_cast<uint4 *>(row + j * 32 * EA)[lane] =
+                    make_uint4(r.w[4 * j], r.w[4 * j + 1], r.w[4 * j + 2], r.w[4 * j + 3]);
+        if (NB && (vm & (1u << NA)))
+            reinterpret_cast<uint2 *>(row + OFF_B)[lane] = make_uint2(r.w[4 * NA], r.w[4 * NA + 1]);
+        if (NC && (vm & (2u << NA))) reinterpret_cast<unsigned *>(row + OFF_C)[lane] = r.w[W - 1];
+    }
+    __device__ static void widen(const Raw &r, float (&v)[E]) {
+        if constexpr (BF16) {
+#pragma unroll
+            for (int i = 0; i < W; i++) {
+                v[2 * i] = __uint_as_float(r.w[i] << 16);
+                v[2 * i + 1] = __uint_as_float(r.w[i] & 0xFFFF0000u);
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < E; i++) v[i] = __uint_as_float(r.w[i]);
+        }
+    }
+    // as stored: BF16 rounds stochastically (one 64-bit draw per four values), FP32 as is
+    __device__ static Raw pack(const float (&v)[E], LaneBits &rb) {
+        Raw r;
+        if constexpr (BF16) {
+#pragma unroll
+            for (int i = 0; i < W; i += 2) {
+                const uint64_t h = rb.next();
+                r.w[i] = pack_sr2(make_float2(v[2 * i], v[2 * i + 1]), h);
+                if (i + 1 < W) r.w[i + 1] = pack_sr2(make_float2(v[2 * i + 2], v[2 * i + 3]), h >> 32);
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < E; i++) r.w[i] = __float_as_uint(v[i]);
+        }
+        return r;
+    }
+    // the lane's part of x . y with four independent partial sums (a chain of ceil(E/4) FMAs)
+    __device__ static float dot(const float (&x)[E], const float (&y)[E]) {
+        float f[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int i = 0; i < E; i++) f[i & 3] = fmaf(x[i], y[i], f[i & 3]);
+        return (f[0] + f[1]) + (f[2] + f[3]);
+    }
+};
+
+template <bool BF16, int E, bool SYNC>
 __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a, int warps) {
-    using S = Store<BF16>;
-    using T = typename S::T;
+    using LR = LaneRow<BF16, E>;
+    using T = typename LR::T;
+    using Raw = typename LR::Raw;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int w = a.window, B = a.batch, ld = a.ld, d = a.d;
+    const int w = a.window, B = a.batch, ld = a.ld;
     const FastMod mod_w((uint32_t) w);
-    const int n4 = (d + 3) >> 2;
     const Layout Lo = make_layout_stream(ld, w, a.negative, B, BF16);
     float *s_exp = reinterpret_cast<float *>(smem_raw);
     FastMod *s_mod_2w = reinterpret_cast<FastMod *>(smem_raw + kExpBytes);
@@ -1126,10 +779,13 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
     unsigned long long *wst = reinterpret_cast<unsigned long long *>(base + Lo.exit_off);
     if (lane == 0)
         for (int i = 0; i < kStreamStats; i++) wst[i] = 0;
+    rep::Stager st = make_stager(base + Lo.bar_off, a.stage_bulk, lane);
     T *w_in = static_cast<T *>(a.w_in);
     T *w_out = static_cast<T *>(a.w_out);
+    const unsigned vm = LR::valid_mask(lane, ld);
     const int epoch = hogwild_epoch(a);
     bool failed = false;
+    unsigned fail_bits = 0;
 
     for (;;) {
         unsigned long long line = 0;
@@ -1153,23 +809,16 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
             // word again) is replaced by the value written.  Each position's b is drawn one
             // position ahead, from the same random stream, so the next position's first context
             // is known in time.  With FP32 tables the raw row is twice the registers, and keeping
-            // it across positions measured 5% slower: there a position reads its first row itself.
-            typename S::Raw yn[NV4];
-            {
-                const T *yrow0 = w_out + (size_t) __ldg(sen) * ld;
-#pragma unroll
-                for (int k = 0; k < NV4; k++) yn[k] = lane + 32 * k < n4 ? S::loadraw_g(yrow0, lane + 32 * k) : S::zero_raw();
-            }
+            // it across positions measured slower: there a position reads its first row itself.
+            Raw yn = LR::load(w_out + (size_t) __ldg(sen) * ld, lane, vm);
             rng = lcg_next(rng);
             int b_next = (int) mod_w(rng);
-            typename S::Raw xn[NV4];
+            Raw xn;
             int c_next = 1, w_next = 0;  // position 0's first context is position 1 (its window starts at 0)
             if constexpr (!SYNC && BF16) {
                 if (L > 1) {
                     w_next = __ldg(sen + 1);
-                    const T *xrow0 = w_in + (size_t) w_next * ld;
-#pragma unroll
-                    for (int k = 0; k < NV4; k++) xn[k] = lane + 32 * k < n4 ? S::loadraw_g(xrow0, lane + 32 * k) : S::zero_raw();
+                    xn = LR::load(w_in + (size_t) w_next * ld, lane, vm);
                 }
             }
             for (int p = 0; p < L; p++) {
@@ -1180,18 +829,14 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                 }
                 const int t = __ldg(sen + p);
                 T *yrow = w_out + (size_t) t * ld;
-                Row<NV4> y;
-#pragma unroll
-                for (int k = 0; k < NV4; k++) y.v[k] = S::widen(yn[k]);
+                float y[E];
+                LR::widen(yn, y);
                 const int t_next = p + 1 < L ? __ldg(sen + p + 1) : t;
-                if (t_next != t) {
-                    const T *ynrow = w_out + (size_t) t_next * ld;
-#pragma unroll
-                    for (int k = 0; k < NV4; k++) yn[k] = lane + 32 * k < n4 ? S::loadraw_g(ynrow, lane + 32 * k) : S::zero_raw();
-                }
+                if (t_next != t) yn = LR::load(w_out + (size_t) t_next * ld, lane, vm);
                 const int lo_c = max(p - w + b, 0), hi_c = min(p + w - b, L - 1);
                 const int n = hi_c - lo_c;
                 if constexpr (SYNC) {
+                    // window-synchronous: every context scored against the same target row
                     for (int i0 = 0; i0 < n; i0 += 2) {
                         float f[2] = {0.f, 0.f};
                         int wd[2] = {-1, -1};
@@ -1200,12 +845,9 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                             if (i0 + u < n) {
                                 const int c = lo_c + i0 + u + (lo_c + i0 + u >= p ? 1 : 0);
                                 wd[u] = __ldg(sen + c);
-                                const T *x = w_in + (size_t) wd[u] * ld;
-#pragma unroll
-                                for (int k = 0; k < NV4; k++) {
-                                    const int cc = lane + 32 * k;
-                                    if (cc < n4) f[u] = f4_dot(S::load4g(x, cc), y.v[k], f[u]);
-                                }
+                                float xv[E];
+                                LR::widen(LR::load(w_in + (size_t) wd[u] * ld, lane, vm), xv);
+                                f[u] = LR::dot(xv, y);
                             }
 #pragma unroll
                         for (int o = 16; o > 0; o >>= 1) {
@@ -1221,7 +863,7 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                                 }
                     }
                     __syncwarp();
-                    if (lane == 0)
+                    if (lane == 0)  // a word twice among the contexts: one update with the summed gradient
                         for (int i = 1; i < n; i++)
                             for (int k = 0; k < i; k++)
                                 if (ctx_w[k] == ctx_w[i]) {
@@ -1230,26 +872,23 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                                     break;
                                 }
                     __syncwarp();
-                    Row<NV4> dy;
+                    float dy[E];
 #pragma unroll
-                    for (int k = 0; k < NV4; k++) dy.v[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    for (int k = 0; k < E; k++) dy[k] = 0.f;
                     for (int i = 0; i < n; i++) {
                         const float g = ctx_g[i];
                         T *x = w_in + (size_t) ctx_w[i] * ld;
+                        float xv[E];
+                        LR::widen(LR::load(x, lane, vm), xv);
 #pragma unroll
-                        for (int k = 0; k < NV4; k++) {
-                            const int cc = lane + 32 * k;
-                            if (cc < n4) {
-                                const float4 xv = S::load4g(x, cc);
-                                dy.v[k] = f4_fma(g, xv, dy.v[k]);
-                                if (g != 0.f) S::store4(x, cc, f4_fma(g, y.v[k], xv), rb.next());
-                            }
+                        for (int k = 0; k < E; k++) {
+                            dy[k] = fmaf(g, xv[k], dy[k]);
+                            xv[k] = fmaf(g, y[k], xv[k]);
                         }
+                        if (g != 0.f) LR::store(x, LR::pack(xv, rb), lane, vm);
                     }
 #pragma unroll
-                    for (int k = 0; k < NV4; k++)
-                        y.v[k] = make_float4(y.v[k].x + dy.v[k].x, y.v[k].y + dy.v[k].y, y.v[k].z + dy.v[k].z,
-                                             y.v[k].w + dy.v[k].w);
+                    for (int k = 0; k < E; k++) y[k] += dy[k];
                 } else if (n > 0) {
                     // contexts c in [lo_c, hi_c] without p, in window order; the first one and its
                     // row were read during the previous position (L > 1 gives every position one)
@@ -1258,9 +897,7 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                     if constexpr (!BF16) {
                         c = lo_c == p ? lo_c + 1 : lo_c;
                         wc = __ldg(sen + c);
-                        const T *xrow0 = w_in + (size_t) wc * ld;
-#pragma unroll
-                        for (int k = 0; k < NV4; k++) xn[k] = lane + 32 * k < n4 ? S::loadraw_g(xrow0, lane + 32 * k) : S::zero_raw();
+                        xn = LR::load(w_in + (size_t) wc * ld, lane, vm);
                     }
                     // the next position's first context: its window start, which is below it
                     // (b_next < w), so never the position itself
@@ -1269,49 +906,35 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                     for (int i = 0; i < n; i++) {
                         const int word = wc;
                         T *x = w_in + (size_t) word * ld;
-                        Row<NV4> xr;
-                        float f = 0.f;
-#pragma unroll
-                        for (int k = 0; k < NV4; k++) {
-                            xr.v[k] = S::widen(xn[k]);
-                            f = f4_dot(xr.v[k], y.v[k], f);
-                        }
+                        float xr[E];
+                        LR::widen(xn, xr);
+                        float f = LR::dot(xr, y);
                         const bool more = i + 1 < n;
                         const bool ahead = more || (BF16 && has_next);
                         if (ahead) {
                             c = more ? (c + 1 == p ? c + 2 : c + 1) : c_first_next;
                             wc = __ldg(sen + c);
-                            if (wc != word) {
-                                const T *xnrow = w_in + (size_t) wc * ld;
-#pragma unroll
-                                for (int k = 0; k < NV4; k++)
-                                    xn[k] = lane + 32 * k < n4 ? S::loadraw_g(xnrow, lane + 32 * k) : S::zero_raw();
-                            }
+                            if (wc != word) xn = LR::load(w_in + (size_t) wc * ld, lane, vm);
                         }
                         f = warp_sum(f);
                         const float g = grad_from_table(f, 1, alpha, s_exp);
-                        const bool again = ahead && wc == word;
+                        float xw[E];
 #pragma unroll
-                        for (int k = 0; k < NV4; k++) {
-                            const int cc = lane + 32 * k;
-                            const float4 yv = y.v[k];
-                            y.v[k] = f4_fma(g, xr.v[k], yv);
-                            const typename S::Raw r = S::pack4(f4_fma(g, yv, xr.v[k]), rb.next());
-                            if (cc < n4) S::storeraw(x, cc, r);
-                            if (again) xn[k] = r;
+                        for (int k = 0; k < E; k++) {
+                            xw[k] = fmaf(g, y[k], xr[k]);
+                            y[k] = fmaf(g, xr[k], y[k]);
                         }
+                        const Raw r = LR::pack(xw, rb);
+                        LR::store(x, r, lane, vm);
+                        if (ahead && wc == word) xn = r;
                     }
                     c_next = c;
                     w_next = wc;
                 }
                 pairs += n;
-#pragma unroll
-                for (int k = 0; k < NV4; k++) {
-                    const int cc = lane + 32 * k;
-                    const typename S::Raw r = S::pack4(y.v[k], rb.next());
-                    if (cc < n4) S::storeraw(yrow, cc, r);
-                    if (t_next == t) yn[k] = r;
-                }
+                const Raw r = LR::pack(y, rb);
+                LR::store(yrow, r, lane, vm);
+                if (t_next == t) yn = r;
             }
             __syncwarp();  // this sentence's row writes before any lane's staging reads
             // ---- repulsion (:571-679) ----
@@ -1324,22 +947,15 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                 const int K = rep_b * a.negative;
                 if (!warp_draw_negatives(a.table, a.vocab, rng, sen, L, K, negs, lane, a.max_resample)) {
                     failed = true;
+                    fail_bits |= kErrResample;
                     break;
                 }
                 batches++;
                 negs_drawn += K;
-                if (K > 0) {
-                    if constexpr (BF16) {
-                        if (Lo.mma)
-                            repel_mma(a, Lo, base, sen + lo_b, rows, negs, K, alpha, s_exp, G, dup, lane, rb);
-                        else
-                            repel_simt<true>(a, Lo, base, sen + lo_b, rows, negs, K, alpha, s_exp, G, dup, lane, rb);
-                    } else {
-                        if (Lo.mma)
-                            repel_mma_f32(a, Lo, base, sen + lo_b, rows, negs, K, alpha, s_exp, G, dup, lane);
-                        else
-                            repel_simt<false>(a, Lo, base, sen + lo_b, rows, negs, K, alpha, s_exp, G, dup, lane, rb);
-                    }
+                if (K > 0 && !repel_batch<BF16>(a, Lo, base, sen + lo_b, rows, negs, K, alpha, s_exp, G, dup, lane, rb, st)) {
+                    failed = true;  // a staging copy did not complete
+                    fail_bits |= kErrStaging;
+                    break;
                 }
                 __syncwarp();
             }
@@ -1358,28 +974,39 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
         atomicAdd(&a.cnt->pairs, wst[2]);
         atomicAdd(&a.cnt->batches, wst[3]);
         atomicAdd(&a.cnt->negatives, wst[4]);
-        if (failed) atomicOr(&a.cnt->error, kErrResample);
+        if (fail_bits) atomicOr(&a.cnt->error, fail_bits);
     }
 }
 
-template <int NV4, bool BF16, bool SYNC>
-cudaError_t launch_stream_nvs(const TrainArgs &a, int grid, int warps, cudaStream_t s) {
+template <bool BF16, int E, bool SYNC>
+cudaError_t launch_stream_e(const TrainArgs &a, int grid, int warps, cudaStream_t s) {
     const Layout Lo = make_layout_stream(a.ld, a.window, a.negative, a.batch, BF16);
     const size_t smem = kSmemHead + (size_t) warps * Lo.per_warp;
-    cudaError_t e = cudaFuncSetAttribute(k_stream_train<NV4, BF16, SYNC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    cudaError_t e = cudaFuncSetAttribute(k_stream_train<BF16, E, SYNC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
     if (e != cudaSuccess) return e;
-    k_stream_train<NV4, BF16, SYNC><<<grid, warps * 32, smem, s>>>(a, warps);
+    k_stream_train<BF16, E, SYNC><<<grid, warps * 32, smem, s>>>(a, warps);
     return cudaGetLastError();
+}
+
+// Elements per lane of the streamed kernel's rows for a hidden size d (d <= 32 E).
+inline int stream_lane_elems(int d) { return d <= 128 ? 4 : d <= 256 ? 8 : d <= 320 ? 10 : d <= 384 ? 12 : 16; }
+
+template <bool BF16, int E>
+cudaError_t launch_stream_es(const TrainArgs &a, int grid, int warps, cudaStream_t s) {
+    return a.sync_window ? launch_stream_e<BF16, E, true>(a, grid, warps, s) : launch_stream_e<BF16, E, false>(a, grid, warps, s);
 }
 
 template <bool BF16>
 cudaError_t launch_stream_mode(const TrainArgs &a, int grid, int warps, cudaStream_t s) {
-    const bool y = a.sync_window;
-    switch ((a.d + 127) / 128) {
-        case 1: return y ? launch_stream_nvs<1, BF16, true>(a, grid, warps, s) : launch_stream_nvs<1, BF16, false>(a, grid, warps, s);
-        case 2: return y ? launch_stream_nvs<2, BF16, true>(a, grid, warps, s) : launch_stream_nvs<2, BF16, false>(a, grid, warps, s);
-        case 3: return y ? launch_stream_nvs<3, BF16, true>(a, grid, warps, s) : launch_stream_nvs<3, BF16, false>(a, grid, warps, s);
-        case 4: return y ? launch_stream_nvs<4, BF16, true>(a, grid, warps, s) : launch_stream_nvs<4, BF16, false>(a, grid, warps, s);
+    if (a.d > 512) return cudaErrorInvalidValue;
+    const int e = a.lane_elems ? a.lane_elems : stream_lane_elems(a.d);
+    if (32 * e < a.d) return cudaErrorInvalidValue;
+    switch (e) {
+        case 4: return launch_stream_es<BF16, 4>(a, grid, warps, s);
+        case 8: return launch_stream_es<BF16, 8>(a, grid, warps, s);
+        case 10: return launch_stream_es<BF16, 10>(a, grid, warps, s);
+        case 12: return launch_stream_es<BF16, 12>(a, grid, warps, s);
+        case 16: return launch_stream_es<BF16, 16>(a, grid, warps, s);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -1405,6 +1032,22 @@ int batched_max_warps(int ld, int window, int negative, int batch, bool bf16, si
     const long cap = stream ? kMaxWarpsS : kMaxWarpsB;
     if (w > cap) w = cap;
     return (int) w;
+}
+
+int batched_ctas_per_sm(int ld, int window, int negative, int batch, bool bf16, bool stream, int warps) {
+    const Layout Lo = stream ? make_layout_stream(ld, window, negative, batch, bf16) : make_layout(ld, window, negative, batch, bf16);
+    const size_t smem = kSmemHead + (size_t) warps * Lo.per_warp + 1024;  // + the CTA's reserved 1 KB
+    const int by_smem = (int) ((228u * 1024u) / smem);
+    const int by_threads = 2048 / (32 * warps);
+    const int by_regs = 65536 / (128 * 32 * warps);
+    return std::min(by_smem, std::min(by_threads, by_regs));
+}
+
+int stream_lane_elems_default(int d) { return stream_lane_elems(d); }
+int stream_lane_elems_next(int e) { return e == 4 ? 8 : e == 8 ? 10 : e == 10 ? 12 : e == 12 ? 16 : 0; }
+
+bool batched_tensor_repulsion(int window, int negative, int batch) {
+    return rep::make_geom(window, negative, batch, true).mma;
 }
 
 cudaError_t launch_batched_train(const TrainArgs &a, bool bf16, bool stream, int grid, int warps_per_cta, cudaStream_t s) {

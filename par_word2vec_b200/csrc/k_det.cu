@@ -9,7 +9,6 @@
 //     oracle's cblas_sgemm fixes), and scatters of duplicate rows apply in the reference's order.
 // The result is bit-identical to the reference built without FMA contraction.
 #include <cstring>
-#include <mutex>
 
 #include "common.cuh"
 #include "internal.h"
@@ -358,9 +357,6 @@ constexpr int kNoAllocMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-std::mutex g_noalloc_mu;
-void *g_noalloc_addr[kNoAllocMaxDevices];  // device address of g_noalloc_scratch, per device
-
 }  // namespace
 
 extern "C" int parw2v_det_train_noalloc(const parw2v_config *cfg, int vocab_size, uint64_t train_words,
@@ -384,17 +380,17 @@ extern "C" int parw2v_det_train_noalloc(const parw2v_config *cfg, int vocab_size
     if (prev != k.device && cudaSetDevice(k.device) != cudaSuccess)
         return set_global_error(PARW2V_ERR_ARG, "device ordinal out of range");
     int rc = PARW2V_OK;
+    // The device address of the array in the current device's context, looked up on every call
+    // (cheap once the module is loaded): an address kept from an earlier call would be stale
+    // after cudaDeviceReset or under another context.  The host-side name g_noalloc_scratch is
+    // not a device address and is never passed to a kernel.
     void *scratch = nullptr;
     {
-        // set-up, once per device with that device current: the device address of the array
-        std::lock_guard<std::mutex> lock(g_noalloc_mu);
-        if (!g_noalloc_addr[k.device]) {
-            void *p = nullptr;
-            const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-            if (e != cudaSuccess) rc = set_global_error(PARW2V_ERR_CUDA, cudaGetErrorString(e));
-            else g_noalloc_addr[k.device] = p;
+        const cudaError_t e = cudaGetSymbolAddress(&scratch, g_noalloc_scratch);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            rc = set_global_error(PARW2V_ERR_CUDA, cudaGetErrorString(e));
         }
-        scratch = g_noalloc_addr[k.device];
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     DevCounters h{};

@@ -49,6 +49,16 @@ __device__ __forceinline__ void ldsm_x2_t(unsigned (&r)[2], const void *p) {
     const unsigned a = (unsigned) __cvta_generic_to_shared(p);
     asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0,%1}, [%2];" : "=r"(r[0]), "=r"(r[1]) : "r"(a));
 }
+__device__ __forceinline__ void ldsm_x2(unsigned (&r)[2], const void *p) {
+    const unsigned a = (unsigned) __cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];" : "=r"(r[0]), "=r"(r[1]) : "r"(a));
+}
+// Inverse of ldsm_x2_t: lane (g, t) holds {M[2t][g], M[2t+1][g]} of two 8x8 BF16 matrices and the
+// lanes 0..15 give the addresses of their rows (lanes 0-7 matrix 0, 8-15 matrix 1).
+__device__ __forceinline__ void stsm_x2_t(void *p, unsigned r0, unsigned r1) {
+    const unsigned a = (unsigned) __cvta_generic_to_shared(p);
+    asm volatile("stmatrix.sync.aligned.m8n8.x2.trans.shared.b16 [%0], {%1, %2};" ::"r"(a), "r"(r0), "r"(r1) : "memory");
+}
 // D += A (16x16 bf16, row) * B (16x8 bf16, col), FP32 accumulate
 __device__ __forceinline__ void mma16816(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
     asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "

@@ -174,6 +174,29 @@ def write_text(path: str, tokens: np.ndarray, lengths: np.ndarray, prefix: str =
     return total
 
 
+def write_stream_text(path: str, stream: np.ndarray, words: list[bytes], chunk: int = 1 << 23) -> int:
+    """Write a vocabulary-id stream (0 = "</s>" ends a line) as reference-readable text: every
+    word followed by a space, a newline per "</s>" (the reference's tokenizer reads the same ids
+    back, PAR_Word2Vec_cpu.cpp:120-144).  Vectorised over chunks of
+    the stream (a gather of the words' bytes), so 10^8 tokens take seconds.  Returns bytes written."""
+    lens = np.array([len(w) + 1 for w in words], dtype=np.int64)  # word + separator
+    lens[0] = 1  # "</s>" is written as the newline alone
+    flat = np.frombuffer(b"".join([b"\n"] + [w + b" " for w in words[1:]]), dtype=np.uint8)
+    starts = np.concatenate([[0], np.cumsum(lens)[:-1]])
+    s = np.asarray(stream)
+    total = 0
+    with open(path, "wb") as f:
+        for c0 in range(0, len(s), chunk):
+            ids = s[c0: c0 + chunk].astype(np.int64)
+            ln = lens[ids]
+            out_start = np.cumsum(ln) - ln
+            src = np.repeat(starts[ids] - out_start, ln) + np.arange(int(ln.sum()), dtype=np.int64)
+            buf = flat[src]  # each word keeps its trailing space, also before a newline
+            f.write(buf.tobytes())
+            total += len(buf)
+    return total
+
+
 def topic_zipf_stream_torch(n_tokens: int, n_types: int, n_topics: int, *, lognormal_mean: float = 25.0,
                             lognormal_sigma: float = 1.0, p_global: float = 0.5, s: float = 1.0, seed: int = 4,
                             min_count: int = 5, device: str = "cuda"):

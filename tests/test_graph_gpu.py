@@ -86,6 +86,10 @@ def test_graph_matches_reference_loss_and_recall(graph_run, mode, variant):
     assert np.isfinite(w_in).all() and np.isfinite(w_out).all()
     assert st["words"] == len(run["stream"])
     assert st["kept"] == int((run["stream"] != 0).sum())  # no subsampling: every node visit trains
+    # window 10 draws up to 19 * 5 = 95 shared negatives per batch: the BATCHED modes still take
+    # the tensor-core repulsion
+    want = pw.REPULSION_SERIAL if mode == pw.MODE_PLAIN else pw.REPULSION_TENSOR
+    assert st["repulsion"] == want
     loss, rec = score(run, w_in, w_out)
     print(f"graph mode {mode} variant {variant}: loss {loss:.5f} (ref mean {ref_loss:.5f} of {run['ref_losses']}) recall {rec:.4f} "
           f"(ref {ref_rec:.4f}) ms {st['kernel_ms']:.1f}")

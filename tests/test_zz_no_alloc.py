@@ -16,12 +16,6 @@ from oracle import pwo
 pytestmark = pytest.mark.gpu
 
 
-class _Stats(ctypes.Structure):
-    _fields_ = [("words", ctypes.c_uint64), ("kept", ctypes.c_uint64), ("sentences", ctypes.c_uint64),
-                ("pairs", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("negatives", ctypes.c_uint64),
-                ("kernel_ms", ctypes.c_double), ("pack_ms", ctypes.c_double), ("final_alpha", ctypes.c_float)]
-
-
 def keep_thresholds(counts, sample, train_words):
     """sqrtf(r) + r with r = (sample * (float) train_words) / (float) count, all in FP32."""
     c = counts.astype(np.float32)
@@ -63,7 +57,7 @@ def test_noalloc_matches_det_entry_point_on_two_calls(golden_cases, case):
     for call in range(2):
         d_in = torch.from_numpy(w0_in).to(dev)
         d_out = torch.zeros((V, d), dtype=torch.float32, device=dev)
-        st = _Stats()
+        st = pw._Stats()  # the library's parw2v_stats layout
         rc = lib.parw2v_det_train_noalloc(ctypes.byref(cfg), V, int(g.counts.sum()), d_corpus.data_ptr(),
                                           len(g.stream) - 1, d_table.data_ptr(), d_exp.data_ptr(),
                                           d_thr.data_ptr(), d_in.data_ptr(), d_out.data_ptr(), d,
