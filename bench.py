@@ -76,6 +76,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the reference CPU leg")
     ap.add_argument("--staging", default="auto", choices=["auto", "bulk", "cpasync"],
                     help="repulsion staging copies (parw2v_config.staging); the result does not depend on it")
+    ap.add_argument("--attraction", default="default", choices=["default", "sequential", "pipelined"],
+                    help="attraction form (parw2v_config.attraction); pipelined = sequential up to rounding")
+    ap.add_argument("--autotune", type=int, default=0, help="parw2v_config.autotune")
     ap.add_argument("--min-rounds", type=int, default=0,
                     help="parw2v_config.min_rounds (0: the library's cap on sentences in flight; -1: no cap, "
                          "as the 800M-token corpus runs uncapped under the default)")
@@ -365,8 +368,11 @@ def main():
     def flush():
         flush_buf.add_(1)  # a 256 MB write: evicts the 126 MB L2
 
+    attraction = {"default": pw.ATTRACT_DEFAULT, "sequential": pw.ATTRACT_SEQUENTIAL,
+                  "pipelined": pw.ATTRACT_PIPELINED}[args.attraction]
+
     def make(m, seed, min_rounds=None, stream=stream_np):
-        t = pw.Trainer(mode=m, device=local, seed=seed, staging=staging,
+        t = pw.Trainer(mode=m, device=local, seed=seed, staging=staging, attraction=attraction, autotune=args.autotune,
                        min_rounds=args.min_rounds if min_rounds is None else min_rounds, **hyper)
         t.set_vocab(counts)
         t.init_weights()
@@ -413,12 +419,13 @@ def main():
     e2e_ms, _ = timed_region(torch, dist, e2e_step, args.steps, flush if l2_resident else None)
     e2e = {"value": words_all / (e2e_ms / 1e3), "unit": "words/s", "h2d_bytes_per_step": 4 * n,
            "d2h_bytes_per_step": 4 * V * d}
-    grid, warps = stats[0]["grid"], stats[0]["warps_per_cta"]
     tr.close()
 
     cfg = static_config(args)
     cfg.update({"corpus_tokens_with_eos": n, "sentences": n_sent, "vocab_size": V, "min_rounds": args.min_rounds,
-                "staging": args.staging, "replicas": world, "launch": {"grid": grid, "warps_per_cta": warps},
+                "staging": args.staging, "attraction": args.attraction, "autotune": args.autotune,
+                "replicas": world, "launch": {k: stats[0][k] for k in ("grid", "warps_per_cta", "lane_elems",
+                                                                        "staging", "attraction", "repulsion")},
                 "l2": ("flushed before every step (256 MB write, outside the timed events); the tables fit in L2"
                        if l2_resident else "no flush: corpus (4 B/token) and weights exceed the 126 MB L2")})
     line = {"metric": METRIC, "value": value, "unit": "words/s", "n_gpus": world, "steps": args.steps,
@@ -513,7 +520,19 @@ def reference_leg(args, pw, evaluate, hyper, dev, tmp, corpus_text, stream_np, c
     ours_loss = score_loss(pw, evaluate, c2, hyper, w_in, w_out, triples)
     ref_loss = score_loss(pw, evaluate, c2, hyper, ref_win, ref_wout, triples)
     words_ref = r["train_words"] * hyper["iter"]
-    return {
+    extra = {}
+    if args.workload == "graph" and os.path.exists(ref_run.GPU_GRAPH_BIN):
+        # the reference's own GPU program on the same walks: the GPU-vs-GPU comparison
+        g = ref_run.run_gpu_graph(corpus, ref_flags(hyper), int(c2[0]))
+        pos = {w: i for i, w in enumerate(g["words"])}
+        g_win = g["win"][np.array([pos[w] for w in w2])]
+        extra["gpu_reference"] = {
+            "value": words_ref / g["elapsed"], "unit": "words/s", "device_s": g["elapsed"],
+            "recall_at_10": evaluate.recall_at_10(g_win, l2, queries, device=dev),
+            "note": "PAR_Word2Vec_gpu_graph.cu built for sm_100a (oracle/Makefile ref-gpu), default -gamma 32, "
+                    "its own CUDA-event time of its training kernel; it draws negatives uniformly and keeps "
+                    "alpha fixed within an epoch, so its loss is not comparable (it saves W_in only)"}
+    return {**extra,
         "cpu_baseline": {"value": words_ref / r["elapsed"], "unit": "words/s", "cores": threads, "kind": "reference",
                          "sample": note + "; words/sec = corpus words x iter / the reference's own Elapsed (its "
                                           "per-thread corpus load + training)",

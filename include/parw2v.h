@@ -71,8 +71,9 @@ typedef struct {
     int autotune;    /* BATCHED modes: 1 = on the first parw2v_train (and whenever the number of
                         sentences in flight changes), time short trials of the launch knobs that
                         do not change the result -- the split of the sentences in flight into CTAs
-                        and warps, the row elements per lane of the streamed kernel and the staging
-                        copies (unless cfg.staging fixes it) -- on a prefix of the first epoch, with
+                        and warps, the row elements per lane of the streamed kernel, the staging
+                        copies (unless cfg.staging fixes them) and, with PARW2V_ATTRACT_DEFAULT, the
+                        sequential attraction's plain or pipelined form -- on a prefix of the first epoch, with
                         the weights restored after each trial, and keep the fastest; 0 = the
                         compiled-in choices */
 } parw2v_config;
@@ -97,6 +98,10 @@ typedef struct {
 #define PARW2V_ATTRACT_WINDOW 2     /* window-synchronous: all contexts of a target are scored
                                        against the same target row, then all updates are applied
                                        (the contexts x d by d x 1 contraction of the window) */
+#define PARW2V_ATTRACT_PIPELINED 3  /* SEQUENTIAL's updates in SEQUENTIAL's order, with the score of
+                                       each next context formed as x'.y + g (x'.x) while the current
+                                       gradient g is looked up (equal up to FP32 rounding).  The
+                                       BATCHED streamed kernel only; DET and PLAIN run SEQUENTIAL */
 
 typedef struct {
     uint64_t words;      /* raw tokens read incl. "</s>" over all epochs: the reference's
@@ -114,6 +119,7 @@ typedef struct {
     int repulsion;       /* PARW2V_REPULSION_* path the training kernel took for the batches */
     int lane_elems;      /* BATCHED streamed kernel: row elements each lane holds */
     int staging;         /* BATCHED modes: PARW2V_STAGING_BULK or _CPASYNC as launched */
+    int attraction;      /* PARW2V_ATTRACT_* form the training kernel ran */
 } parw2v_stats;
 
 /* parw2v_stats.repulsion */

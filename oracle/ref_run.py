@@ -1,5 +1,7 @@
-"""TEST INFRASTRUCTURE ONLY: runs the reference binary built from PAR_Word2Vec_cpu.cpp by
-oracle/Makefile (oracle/_ref/par_w2v_ref_fast) and reads back what its driver dumps.
+"""TEST INFRASTRUCTURE ONLY: runs the reference binaries built by oracle/Makefile -- the CPU
+program PAR_Word2Vec_cpu.cpp (oracle/_ref/par_w2v_ref_fast, through its dumping driver) and the GPU
+graph program PAR_Word2Vec_gpu_graph.cu (oracle/_ref/par_w2v_gpu_graph) -- and reads back their
+outputs.
 
 Only tests/ and bench.py's CPU-baseline / reference legs use this module, as the checker and the
 timed CPU baseline; nothing in the library imports it.
@@ -61,3 +63,43 @@ def rows_in_order(ref: dict, words: list[bytes]):
     pos = {w: i for i, w in enumerate(ref["words"])}
     idx = np.array([pos[w] for w in words], dtype=np.int64)
     return ref["win"][idx], ref["wout"][idx]
+
+
+GPU_GRAPH_BIN = os.path.join(os.path.dirname(pwo.REF_FAST_BIN), "par_w2v_gpu_graph")
+
+
+def read_binary_vectors(path: str):
+    """A saveModel file written with -binary 1 (PAR_Word2Vec_gpu_graph.cu saveModel): a "V d" header
+    line, then per word its string, a space, d float32 values and a newline."""
+    data = open(path, "rb").read()
+    nl = data.index(b"\n")
+    V, d = map(int, data[:nl].split())
+    pos, words = nl + 1, []
+    W = np.empty((V, d), np.float32)
+    for i in range(V):
+        sp = data.index(b" ", pos)
+        words.append(data[pos:sp])
+        W[i] = np.frombuffer(data, np.float32, d, sp + 1)
+        pos = sp + 1 + 4 * d + 1
+    return words, W
+
+
+def run_gpu_graph(corpus: str, flags: dict, n_sentences: int) -> dict:
+    """One run of the reference's GPU graph program (hidden size 128 only: its kernel reads four
+    32-wide slices of each row) on the first visible device, in this process's environment.
+    Returns its device time ``elapsed`` (its own CUDA-event Elapsed,
+    PAR_Word2Vec_gpu_graph.cu:869-957), W_in and the words in its row order."""
+    if not os.path.exists(GPU_GRAPH_BIN):
+        raise FileNotFoundError(f"{GPU_GRAPH_BIN} is not built (make -C oracle ref-gpu)")
+    with tempfile.TemporaryDirectory() as tmp:
+        out = os.path.join(tmp, "o.bin")
+        # -max-num-sen sizes its host array of sentence offsets: at least the corpus's lines
+        args = [GPU_GRAPH_BIN, "-train", corpus, "-output", out, "-binary", "1", "-debug", "0",
+                "-max-num-sen", str(n_sentences + 16)]
+        for k, v in flags.items():
+            args += ["-" + k.replace("_", "-"), str(v)]
+        subprocess.run(args, check=True, cwd=tmp, stdout=subprocess.DEVNULL)
+        elapsed = float(re.search(rb"Elapsed\s+([0-9.]+)",
+                                  open(os.path.join(tmp, "PAR_Word2Vec_gpu_time"), "rb").read()).group(1))
+        words, W = read_binary_vectors(out)
+    return dict(elapsed=elapsed, words=words, win=W)

@@ -23,7 +23,7 @@ MODE_NAMES = {"det": MODE_DET, "plain": MODE_PLAIN, "batched": MODE_BATCHED, "ba
 TABLE_SIZE = 100_000_000
 EXP_TABLE_SIZE = 1000
 
-ATTRACT_DEFAULT, ATTRACT_SEQUENTIAL, ATTRACT_WINDOW = 0, 1, 2
+ATTRACT_DEFAULT, ATTRACT_SEQUENTIAL, ATTRACT_WINDOW, ATTRACT_PIPELINED = 0, 1, 2, 3
 VARIANT_AUTO, VARIANT_WINDOW, VARIANT_STREAM = 0, 1, 2
 STAGING_AUTO, STAGING_BULK, STAGING_CPASYNC = 0, 1, 2
 REPULSION_SERIAL, REPULSION_TENSOR, REPULSION_CUDA = 0, 1, 2
@@ -61,7 +61,7 @@ class _Stats(ctypes.Structure):
                 ("pairs", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("negatives", ctypes.c_uint64),
                 ("kernel_ms", ctypes.c_double), ("pack_ms", ctypes.c_double), ("final_alpha", ctypes.c_float),
                 ("grid", ctypes.c_int), ("warps_per_cta", ctypes.c_int), ("repulsion", ctypes.c_int),
-                ("lane_elems", ctypes.c_int), ("staging", ctypes.c_int)]
+                ("lane_elems", ctypes.c_int), ("staging", ctypes.c_int), ("attraction", ctypes.c_int)]
 
 
 class _Trace(ctypes.Structure):

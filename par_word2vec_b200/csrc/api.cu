@@ -63,7 +63,7 @@ struct parw2v_ctx {
     struct {
         bool done = false;
         uint64_t inflight = 0;
-        int grid = 0, warps = 0, stage_bulk = 1, lane_elems = 0;
+        int grid = 0, warps = 0, stage_bulk = 1, lane_elems = 0, attr_pipe = 0;
     } tuned;
 };
 
@@ -170,7 +170,7 @@ int parw2v_create(const parw2v_config *cfg, parw2v_ctx **out) {
         return fail(nullptr, PARW2V_ERR_ARG, "invalid configuration value");
     if (k.variant < PARW2V_VARIANT_AUTO || k.variant > PARW2V_VARIANT_STREAM)
         return fail(nullptr, PARW2V_ERR_ARG, "invalid kernel variant");
-    if (k.attraction < PARW2V_ATTRACT_DEFAULT || k.attraction > PARW2V_ATTRACT_WINDOW)
+    if (k.attraction < PARW2V_ATTRACT_DEFAULT || k.attraction > PARW2V_ATTRACT_PIPELINED)
         return fail(nullptr, PARW2V_ERR_ARG, "invalid attraction variant");
     if (k.staging < PARW2V_STAGING_AUTO || k.staging > PARW2V_STAGING_CPASYNC)
         return fail(nullptr, PARW2V_ERR_ARG, "invalid staging method");
@@ -590,7 +590,7 @@ static int autotune(parw2v_ctx *c, TrainArgs a, int base_grid, int base_warps) {
     const parw2v_config &k = c->cfg;
     c->tuned = {};
     struct Cand {
-        int grid, warps, bulk, elems;
+        int grid, warps, bulk, elems, pipe;
     };
     std::vector<std::pair<int, int>> splits = {{base_grid, base_warps}};
     for (int f : {2, 4})
@@ -607,10 +607,14 @@ static int autotune(parw2v_ctx *c, TrainArgs a, int base_grid, int base_warps) {
     if (k.staging != PARW2V_STAGING_AUTO) bulks = {k.staging != PARW2V_STAGING_CPASYNC ? 1 : 0};
     else if (batched_tensor_repulsion(k.window, k.negative, k.batch_size)) bulks = {1, 0};
     else bulks = {1};
+    // the sequential attraction in its plain or pipelined form, unless cfg.attraction fixes one
+    std::vector<int> pipes = {a.attr_pipe};
+    if (stream && k.attraction == PARW2V_ATTRACT_DEFAULT) pipes = {0, 1};
     std::vector<Cand> cands;
     for (auto &sp : splits)
         for (int e : elems)
-            for (int b : bulks) cands.push_back({sp.first, sp.second, b, e});
+            for (int b : bulks)
+                for (int pp : pipes) cands.push_back({sp.first, sp.second, b, e, pp});
     // epoch 0's packed corpus
     CK(c, cudaMemsetAsync(&c->d_cnt->work, 0, sizeof(unsigned long long), c->stream), "autotune");
     CK(c, launch_pack(a, c->d_packed, c->d_line_end, c->d_tile_kept, c->d_tile_zero, pack_tiles(c->n_tokens), c->stream),
@@ -639,6 +643,7 @@ static int autotune(parw2v_ctx *c, TrainArgs a, int base_grid, int base_warps) {
         const Cand &cd = cands[i];
         a.stage_bulk = cd.bulk;
         a.lane_elems = cd.elems;
+        a.attr_pipe = cd.pipe;
         float ms = 0.f;
         for (int pass = 0; pass < 2 && e == cudaSuccess; pass++) {
             DevCounters hc = h0;
@@ -668,6 +673,7 @@ static int autotune(parw2v_ctx *c, TrainArgs a, int base_grid, int base_warps) {
     c->tuned.warps = best.warps;
     c->tuned.stage_bulk = best.bulk;
     c->tuned.lane_elems = best.elems;
+    c->tuned.attr_pipe = best.pipe;
     return PARW2V_OK;
 }
 
@@ -720,6 +726,7 @@ static int train_hogwild(parw2v_ctx *c, TrainArgs &a, parw2v_stats *st) {
             warps = c->tuned.warps;
             a.stage_bulk = c->tuned.stage_bulk;
             a.lane_elems = c->tuned.lane_elems;
+            a.attr_pipe = c->tuned.attr_pipe;
         }
     }
     c->last_grid = grid;
@@ -801,6 +808,8 @@ static int train_hogwild(parw2v_ctx *c, TrainArgs &a, parw2v_stats *st) {
         st->warps_per_cta = warps;
         st->lane_elems = plain ? 0 : (a.lane_elems ? a.lane_elems : (stream_variant(c) ? stream_lane_elems_default(c->cfg.size) : 0));
         st->staging = plain ? 0 : (a.stage_bulk ? PARW2V_STAGING_BULK : PARW2V_STAGING_CPASYNC);
+        st->attraction = a.sync_window ? PARW2V_ATTRACT_WINDOW
+                                       : (!plain && a.attr_pipe ? PARW2V_ATTRACT_PIPELINED : PARW2V_ATTRACT_SEQUENTIAL);
         st->repulsion = plain ? PARW2V_REPULSION_SERIAL
                               : (batched_tensor_repulsion(c->cfg.window, c->cfg.negative, c->cfg.batch_size)
                                      ? PARW2V_REPULSION_TENSOR
@@ -861,6 +870,7 @@ int parw2v_train(parw2v_ctx *c, parw2v_stats *st) {
     a.max_resample = 1LL << 20;
     a.sync_window = c->cfg.attraction == PARW2V_ATTRACT_WINDOW;
     a.stage_bulk = c->cfg.staging != PARW2V_STAGING_CPASYNC;
+    a.attr_pipe = c->cfg.attraction == PARW2V_ATTRACT_PIPELINED;
     if (c->cfg.mode == PARW2V_MODE_DET) return train_det(c, a, st);
     rc = ensure_packing(c);
     if (rc) return rc;

@@ -41,6 +41,26 @@ __host__ __device__ inline uint64_t lcg_jump(uint64_t x, uint64_t n) {
     return acc.a * x + acc.c;
 }
 
+// The affine maps of 0..32 LCG steps, for the jumps of the negative draws (at most 32 draws a
+// round): kLcgJump.a[n] * x + kLcgJump.c[n] is x after n steps.
+struct LcgJumpTable {
+    uint64_t a[33], c[33];
+};
+constexpr LcgJumpTable make_lcg_jump_table() {
+    LcgJumpTable t{};
+    t.a[0] = 1ULL;
+    t.c[0] = 0ULL;
+    for (int n = 1; n <= 32; n++) {
+        t.a[n] = 25214903917ULL * t.a[n - 1];
+        t.c[n] = 25214903917ULL * t.c[n - 1] + 11ULL;
+    }
+    return t;
+}
+static __device__ const LcgJumpTable kLcgJump = make_lcg_jump_table();
+__device__ __forceinline__ uint64_t lcg_jump_small(uint64_t x, int n) {  // 0 <= n <= 32
+    return __ldg(&kLcgJump.a[n]) * x + __ldg(&kLcgJump.c[n]);
+}
+
 // x mod m for a 64-bit x and 0 < m < 2^16, exactly, through 32-bit remainders:
 // (hi * 2^32 + lo) mod m = ((hi mod m) * (2^32 mod m) + lo mod m) mod m, all terms < 2^32.
 __host__ __device__ __forceinline__ uint32_t mod_small(uint64_t x, uint32_t m) {
@@ -91,6 +111,20 @@ __device__ __forceinline__ float warp_sum(float v) {
     return v;
 }
 
+// Two warp sums at once: lanes 0-15 reduce p while lanes 16-31 reduce q, then the halves swap
+// results; every lane ends with the same P = sum(p) and Q = sum(q) (butterfly additions are
+// commutative pairs, so all lanes hold bit-identical sums).  Seven shuffles for two sums.
+__device__ __forceinline__ void warp_sum2(float p, float q, int lane, float &P, float &Q) {
+    const bool hi = lane & 16;
+    float v = hi ? q : p;
+    v += __shfl_xor_sync(0xffffffffu, hi ? p : q, 16);
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const float other = __shfl_xor_sync(0xffffffffu, v, 16);
+    P = hi ? other : v;
+    Q = hi ? v : other;
+}
+
 // Fire-and-forget vector reduction into global memory (sm_90+): one L2 atomic per 8 bytes.
 __device__ __forceinline__ void red_add_f2(float *addr, float2 v) {
     asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(addr), "f"(v.x), "f"(v.y) : "memory");
@@ -114,7 +148,7 @@ static __device__ __noinline__ bool warp_draw_negatives(const int32_t *table, in
         const int nk = min(K - k0, 32);
         int cand = -1;
         if (lane < nk) {
-            const uint64_t r = lcg_jump(rng, (uint64_t) lane + 1);
+            const uint64_t r = lcg_jump_small(rng, lane + 1);
             cand = __ldg(table + (r >> 16) % (uint64_t) kTableSize);
             if (!cand) cand = (int) (r % (uint64_t) (vocab - 1) + 1);
         }
@@ -124,11 +158,11 @@ static __device__ __noinline__ bool warp_draw_negatives(const int32_t *table, in
         const int first = m ? __ffs(m) - 1 : nk;
         if (lane < first) negs[k0 + lane] = cand;
         if (first == nk) {
-            rng = lcg_jump(rng, (uint64_t) nk);
+            rng = lcg_jump_small(rng, nk);
             k0 += nk;
             continue;
         }
-        rng = lcg_jump(rng, (uint64_t) first + 1);
+        rng = lcg_jump_small(rng, first + 1);
         int s = 0;
         for (int64_t tries = 0;; tries++) {
             if (tries >= max_resample) return false;

@@ -57,6 +57,7 @@ struct TrainArgs {
     int sync_window;         // window-synchronous attraction (PARW2V_ATTRACT_WINDOW)
     int stage_bulk;          // BATCHED repulsion staging: 1 bulk copies (TMA unit), 0 16-byte cp.async
     int lane_elems;          // streamed kernel: row elements per lane (0 = the smallest that holds d)
+    int attr_pipe;           // streamed kernel: sequential attraction in its pipelined form
 };
 
 // Launchers (return a cudaError_t)

@@ -748,8 +748,12 @@ struct LaneRow {
     }
 };
 
-template <bool BF16, int E, bool SYNC>
+// ATT: 0 the reference's sequential attraction; 1 window-synchronous; 2 sequential, pipelined (the
+// same updates in the same order, with each pair's dot products taken before the previous pair's
+// gradient is known).
+template <bool BF16, int E, int ATT>
 __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a, int warps) {
+    constexpr bool SYNC = ATT == 1;
     using LR = LaneRow<BF16, E>;
     using T = typename LR::T;
     using Raw = typename LR::Raw;
@@ -903,6 +907,59 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                     // (b_next < w), so never the position itself
                     const bool has_next = p + 1 < L;
                     const int c_first_next = max(p + 1 - w + b_next, 0);
+                    if constexpr (ATT == 2) {
+                        // f_{i+1} = x_{i+1} . y_i = x_{i+1} . y_{i-1} + g_i (x_{i+1} . x_i): both dot
+                        // products and their warp sums are formed while g_i is looked up, so one
+                        // scalar FMA and the table lookup are all that each pair waits for.  The
+                        // row of pair i+2 is read after pair i's store; a pair whose word repeats the
+                        // previous pair's uses the value just stored and the sequential form.
+                        int word = wc;
+                        float xr[E];
+                        LR::widen(xn, xr);
+                        float f = warp_sum(LR::dot(xr, y));
+                        if (1 < n || (BF16 && has_next)) {
+                            c = 1 < n ? (c + 1 == p ? c + 2 : c + 1) : c_first_next;
+                            wc = __ldg(sen + c);
+                            if (wc != word) xn = LR::load(w_in + (size_t) wc * ld, lane, vm);
+                        }
+                        for (int i = 0; i < n; i++) {
+                            const float g = grad_from_table(f, 1, alpha, s_exp);
+                            const bool more = i + 1 < n;
+                            const int word1 = wc;
+                            float x1[E], P = 0.f, Q = 0.f;
+                            if (more) {
+                                LR::widen(xn, x1);
+                                warp_sum2(LR::dot(x1, y), LR::dot(x1, xr), lane, P, Q);
+                            }
+                            T *x = w_in + (size_t) word * ld;
+                            float xw[E];
+#pragma unroll
+                            for (int k = 0; k < E; k++) {
+                                xw[k] = fmaf(g, y[k], xr[k]);
+                                y[k] = fmaf(g, xr[k], y[k]);
+                            }
+                            const Raw r = LR::pack(xw, rb);
+                            LR::store(x, r, lane, vm);
+                            if (i + 2 < n || (BF16 && has_next && more)) {
+                                c = i + 2 < n ? (c + 1 == p ? c + 2 : c + 1) : c_first_next;
+                                wc = __ldg(sen + c);
+                                if (wc != word1) xn = LR::load(w_in + (size_t) wc * ld, lane, vm);
+                            }
+                            if (more) {
+                                if (word1 == word) {
+                                    LR::widen(r, x1);
+                                    f = warp_sum(LR::dot(x1, y));
+                                } else {
+                                    f = fmaf(g, Q, P);
+                                }
+#pragma unroll
+                                for (int k = 0; k < E; k++) xr[k] = x1[k];
+                                word = word1;
+                            } else if (BF16 && has_next && wc == word) {
+                                xn = r;  // the next position's first context is this row, just stored
+                            }
+                        }
+                    } else {
                     for (int i = 0; i < n; i++) {
                         const int word = wc;
                         T *x = w_in + (size_t) word * ld;
@@ -927,6 +984,7 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                         const Raw r = LR::pack(xw, rb);
                         LR::store(x, r, lane, vm);
                         if (ahead && wc == word) xn = r;
+                    }
                     }
                     c_next = c;
                     w_next = wc;
@@ -978,13 +1036,13 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
     }
 }
 
-template <bool BF16, int E, bool SYNC>
+template <bool BF16, int E, int ATT>
 cudaError_t launch_stream_e(const TrainArgs &a, int grid, int warps, cudaStream_t s) {
     const Layout Lo = make_layout_stream(a.ld, a.window, a.negative, a.batch, BF16);
     const size_t smem = kSmemHead + (size_t) warps * Lo.per_warp;
-    cudaError_t e = cudaFuncSetAttribute(k_stream_train<BF16, E, SYNC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    cudaError_t e = cudaFuncSetAttribute(k_stream_train<BF16, E, ATT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
     if (e != cudaSuccess) return e;
-    k_stream_train<BF16, E, SYNC><<<grid, warps * 32, smem, s>>>(a, warps);
+    k_stream_train<BF16, E, ATT><<<grid, warps * 32, smem, s>>>(a, warps);
     return cudaGetLastError();
 }
 
@@ -993,7 +1051,8 @@ inline int stream_lane_elems(int d) { return d <= 128 ? 4 : d <= 256 ? 8 : d <= 
 
 template <bool BF16, int E>
 cudaError_t launch_stream_es(const TrainArgs &a, int grid, int warps, cudaStream_t s) {
-    return a.sync_window ? launch_stream_e<BF16, E, true>(a, grid, warps, s) : launch_stream_e<BF16, E, false>(a, grid, warps, s);
+    if (a.sync_window) return launch_stream_e<BF16, E, 1>(a, grid, warps, s);
+    return a.attr_pipe ? launch_stream_e<BF16, E, 2>(a, grid, warps, s) : launch_stream_e<BF16, E, 0>(a, grid, warps, s);
 }
 
 template <bool BF16>

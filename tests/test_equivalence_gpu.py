@@ -23,9 +23,11 @@ def run(golden, mode, attraction=pw.ATTRACT_SEQUENTIAL, variant=pw.VARIANT_AUTO,
 
 
 @pytest.mark.parametrize("variant", [pw.VARIANT_WINDOW, pw.VARIANT_STREAM])
-@pytest.mark.parametrize("attraction", [pw.ATTRACT_SEQUENTIAL, pw.ATTRACT_WINDOW])
+@pytest.mark.parametrize("attraction", [pw.ATTRACT_SEQUENTIAL, pw.ATTRACT_WINDOW, pw.ATTRACT_PIPELINED])
 @pytest.mark.parametrize("case", ["text_small", "graph_small", "edge", "d100"])
 def test_batched_fp32_equals_plain_sequentially(golden_cases, case, attraction, variant):
+    """PIPELINED (streamed kernel) computes SEQUENTIAL's updates: PLAIN, which runs SEQUENTIAL
+    for it, is the reference for both."""
     g = golden_cases[case]
     sp, (pi, po) = run(g, pw.MODE_PLAIN, attraction)
     sb, (bi, bo) = run(g, pw.MODE_BATCHED, attraction, variant)
@@ -39,7 +41,7 @@ def test_batched_fp32_equals_plain_sequentially(golden_cases, case, attraction, 
 
 
 @pytest.mark.parametrize("variant", [pw.VARIANT_WINDOW, pw.VARIANT_STREAM])
-@pytest.mark.parametrize("attraction", [pw.ATTRACT_SEQUENTIAL, pw.ATTRACT_WINDOW])
+@pytest.mark.parametrize("attraction", [pw.ATTRACT_SEQUENTIAL, pw.ATTRACT_WINDOW, pw.ATTRACT_PIPELINED])
 @pytest.mark.parametrize("case", ["text_small", "d100"])
 def test_batched_bf16_tracks_plain_sequentially(golden_cases, case, attraction, variant):
     """BF16 tables with stochastic rounding (and, for these shapes, the tensor-core repulsion)
