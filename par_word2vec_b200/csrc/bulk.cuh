@@ -42,6 +42,18 @@ __device__ __forceinline__ void bulk_load(void *dst_smem, const void *src_gmem, 
                  "l"(src_gmem), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
 }
+// shared -> global, in the thread's current bulk async-group
+__device__ __forceinline__ void bulk_store(void *dst_gmem, const void *src_smem, unsigned bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst_gmem),
+                 "r"(smem_u32(src_smem)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// this thread's bulk stores have read their shared-memory sources (the staging may be reused)
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// this thread's bulk stores are complete in global memory
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
 // Orders this thread's generic-proxy accesses before its later async-proxy (bulk copy) accesses,
 // and the other way round: shared memory rewritten by the bulk unit after being read by ldmatrix,
 // global rows written by plain stores and then read by bulk copies.

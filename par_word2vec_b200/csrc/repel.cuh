@@ -12,7 +12,8 @@
 //           one-chunk read-to-write window like the reference's unsynchronised `+=`), form the new
 //           values on the tensor cores and store them back.
 // Staging is one bulk copy (cp.async.bulk, the TMA unit) per row and chunk completing on the
-// warp's mbarrier, or, selectable for comparison, 16-byte cp.async copies.  Rows of the tables are
+// warp's mbarrier, and the BF16 write-back one bulk store per row and chunk; or, selectable for
+// comparison, 16-byte cp.async copies and 16-byte stores.  Rows of the tables are
 // never read through this SM's L1 (bulk copies and cp.async.cg read at L2): L1 is not coherent
 // with the other SMs' writes.
 #pragma once
@@ -92,7 +93,9 @@ __device__ __forceinline__ bool stage_rows(Stager &st, const T *w_in, const T *w
     const unsigned bytes = (unsigned) ncols * (unsigned) sizeof(T);
     bool ok = true;
     if (st.bulk) {
-        // earlier generic accesses of the staging (ldmatrix, stmatrix, zeroing) before the bulk writes
+        // the previous chunk's bulk stores have read the staging; earlier generic accesses of the
+        // staging (ldmatrix, stmatrix, zeroing) come before the bulk writes
+        bulk_wait_read_all();
         fence_proxy_async_shared();
         __syncwarp();
         if (lane == 0) mbar_arrive_expect_tx(st.bar, (unsigned) (rows + nk) * bytes);
@@ -399,16 +402,37 @@ __device__ __noinline__ bool repel_bf16(const TrainArgs &a, const Geom &geo, uns
                 }
         }
         __syncwarp();
-        // every distinct row's new chunk back to its table in 16-byte pieces
-        const int psh = ncols == 32 ? 2 : 1;  // pieces per row: ncols / 8
-        for (int it = lane; it < (rows + K) << psh; it += 32) {
-            const int rr = it >> psh, pc = it & ((1 << psh) - 1);
-            const bool is_in = rr < rows;
-            if (dup[is_in ? K + rr : rr - rows] >= 0) continue;
-            const T *src = (is_in ? sin + (size_t) rr * kStride : sout + (size_t) (rr - rows) * kStride) + pc * 8;
-            T *dst = (is_in ? w_in + (size_t) sbw[rr] * ld : w_out + (size_t) negs[rr - rows] * ld) + col0 + pc * 8;
-            *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(src);
+        // every distinct row's new chunk back to its table
+        if (st.bulk) {
+            // one bulk store per row; the next staging waits until they have read the tile
+            fence_proxy_async_shared();  // this lane's stmatrix writes before the bulk reads
+            __syncwarp();
+            for (int rr = lane; rr < rows + K; rr += 32) {
+                const bool is_in = rr < rows;
+                if (dup[is_in ? K + rr : rr - rows] >= 0) continue;
+                const T *src = is_in ? sin + (size_t) rr * kStride : sout + (size_t) (rr - rows) * kStride;
+                T *dst = (is_in ? w_in + (size_t) sbw[rr] * ld : w_out + (size_t) negs[rr - rows] * ld) + col0;
+                bulk_store(dst, src, (unsigned) ncols * 2u);
+            }
+            bulk_commit();
+        } else {
+            const int psh = ncols == 32 ? 2 : 1;  // 16-byte pieces per row: ncols / 8
+            for (int it = lane; it < (rows + K) << psh; it += 32) {
+                const int rr = it >> psh, pc = it & ((1 << psh) - 1);
+                const bool is_in = rr < rows;
+                if (dup[is_in ? K + rr : rr - rows] >= 0) continue;
+                const T *src = (is_in ? sin + (size_t) rr * kStride : sout + (size_t) (rr - rows) * kStride) + pc * 8;
+                T *dst = (is_in ? w_in + (size_t) sbw[rr] * ld : w_out + (size_t) negs[rr - rows] * ld) + col0 + pc * 8;
+                *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(src);
+            }
         }
+        __syncwarp();
+    }
+    if (st.bulk) {
+        // the rows are in global memory before this warp reads them again (the next batch's bulk
+        // copies, the next sentence's plain loads)
+        bulk_wait_all();
+        fence_proxy_async_global();
         __syncwarp();
     }
     return true;
