@@ -74,8 +74,9 @@ typedef struct {
                         and warps, the row elements per lane of the streamed kernel, the staging
                         copies (unless cfg.staging fixes them) and, with PARW2V_ATTRACT_DEFAULT, the
                         sequential attraction's plain or pipelined form -- on a prefix of the first epoch, with
-                        the weights restored after each trial, and keep the fastest; 0 = the
-                        compiled-in choices */
+                        the weights restored after each trial, and keep the fastest (with the
+                        environment variable PARW2V_AUTOTUNE_LOG set, each trial's time is printed
+                        on stderr); 0 = the compiled-in choices */
 } parw2v_config;
 
 /* Repulsion staging of the BATCHED modes (cfg.staging); the result does not depend on it */

@@ -639,6 +639,8 @@ static int autotune(parw2v_ctx *c, TrainArgs a, int base_grid, int base_warps) {
     if (e == cudaSuccess) e = copy((char *) backup + wbytes, c->d_w_out);
     float best_ms = 0.f;
     Cand best = cands[0];
+    // PARW2V_AUTOTUNE_LOG set: every trial's time on stderr (diagnostics; the choice is the same)
+    const bool log_trials = getenv("PARW2V_AUTOTUNE_LOG") != nullptr;
     for (size_t i = 0; i < cands.size() && e == cudaSuccess; i++) {
         const Cand &cd = cands[i];
         a.stage_bulk = cd.bulk;
@@ -658,6 +660,12 @@ static int autotune(parw2v_ctx *c, TrainArgs a, int base_grid, int base_warps) {
             if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
             if (e == cudaSuccess && pass == 1) e = cudaEventElapsedTime(&ms, c->ev0, c->ev1);
         }
+        if (e == cudaSuccess && log_trials)
+            fprintf(stderr, "parw2v autotune: grid %d x %d warps, %d elements per lane, staging %s, attraction %s: "
+                            "%.3f ms for %llu lines\n",
+                    cd.grid, cd.warps, cd.elems ? cd.elems : stream_lane_elems_default(k.size),
+                    cd.bulk ? "bulk" : "cp.async", cd.pipe ? "pipelined" : "sequential", ms,
+                    (unsigned long long) trial);
         if (e == cudaSuccess && (i == 0 || ms < best_ms)) {
             best_ms = ms;
             best = cd;
