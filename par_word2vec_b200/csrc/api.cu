@@ -63,7 +63,7 @@ struct parw2v_ctx {
     struct {
         bool done = false;
         uint64_t inflight = 0;
-        int grid = 0, warps = 0, stage_bulk = 1, lane_elems = 0, attr_pipe = 0;
+        int grid = 0, warps = 0, stage_bulk = 0, lane_elems = 0, attr_pipe = 0;
     } tuned;
 };
 
@@ -604,9 +604,9 @@ static int autotune(parw2v_ctx *c, TrainArgs a, int base_grid, int base_warps) {
         if (e1) elems.push_back(e1);
     }
     std::vector<int> bulks;
-    if (k.staging != PARW2V_STAGING_AUTO) bulks = {k.staging != PARW2V_STAGING_CPASYNC ? 1 : 0};
-    else if (batched_tensor_repulsion(k.window, k.negative, k.batch_size)) bulks = {1, 0};
-    else bulks = {1};
+    if (k.staging != PARW2V_STAGING_AUTO) bulks = {k.staging == PARW2V_STAGING_BULK ? 1 : 0};
+    else if (batched_tensor_repulsion(k.window, k.negative, k.batch_size)) bulks = {0, 1};
+    else bulks = {0};
     // the sequential attraction in its plain or pipelined form, unless cfg.attraction fixes one
     std::vector<int> pipes = {a.attr_pipe};
     if (stream && k.attraction == PARW2V_ATTRACT_DEFAULT) pipes = {0, 1};
@@ -877,7 +877,7 @@ int parw2v_train(parw2v_ctx *c, parw2v_stats *st) {
     a.line_end = c->d_line_end;
     a.max_resample = 1LL << 20;
     a.sync_window = c->cfg.attraction == PARW2V_ATTRACT_WINDOW;
-    a.stage_bulk = c->cfg.staging != PARW2V_STAGING_CPASYNC;
+    a.stage_bulk = c->cfg.staging == PARW2V_STAGING_BULK;
     a.attr_pipe = c->cfg.attraction == PARW2V_ATTRACT_PIPELINED;
     if (c->cfg.mode == PARW2V_MODE_DET) return train_det(c, a, st);
     rc = ensure_packing(c);

@@ -3,6 +3,8 @@
 * ``recall_at_10``  -- planted-cluster recall@10: for each query word, the fraction of its 10
   cosine-nearest neighbours in W_in (excluding itself and "</s>") that carry the query's
   planted label.  Chance level is 1 / number of labels.
+* ``topic_margin`` -- cosine to the query's planted-topic centroid minus the mean cosine to the
+  other centroids: continuous, where recall@10 of these corpora saturates near 1.
 * ``eval_triples`` / ``sgns_loss`` -- a fixed, seeded evaluation set of (target, context,
   negatives) windows drawn from a corpus, scored with the library's FP64 loss kernel.
 
@@ -58,6 +60,41 @@ def recall_at_10(w_in: np.ndarray, labels: np.ndarray, queries: np.ndarray, k: i
         nn = np.argpartition(-sim, k, axis=1)[:, :k]
         hits += int((labels[nn] == labels[q][:, None]).sum())
     return hits / (len(queries) * k)
+
+
+def topic_margin(w_in: np.ndarray, labels: np.ndarray, queries: np.ndarray, device: str | None = None) -> float:
+    """A continuous measure of the planted structure that does not saturate like recall@10: the
+    mean over the queries of cos(q, own topic's centroid) minus the mean cos(q, other topics'
+    centroids), with centroids the normalised means of the unit vectors of all labelled words."""
+    valid = labels >= 0
+    n_lab = int(labels.max()) + 1
+    try:
+        import torch
+        use_torch = device is not None and torch.cuda.is_available()
+    except Exception:
+        use_torch = False
+    if use_torch:
+        import torch
+        W = torch.from_numpy(np.ascontiguousarray(w_in, np.float32)).to(device)
+        W = W / W.norm(dim=1, keepdim=True).clamp_min(1e-12)
+        lab = torch.from_numpy(labels).to(device)
+        idx = torch.from_numpy(np.flatnonzero(valid)).to(device)
+        C = torch.zeros(n_lab, W.shape[1], device=device).index_add_(0, lab[idx], W[idx])
+        C = C / C.norm(dim=1, keepdim=True).clamp_min(1e-12)
+        q = torch.from_numpy(queries.astype(np.int64)).to(device)
+        S = W[q] @ C.T
+        own = S.gather(1, lab[q][:, None]).squeeze(1)
+        other = (S.sum(dim=1) - own) / (n_lab - 1)
+        return float((own - other).mean().item())
+    W = np.asarray(w_in, np.float32)
+    W = W / np.maximum(np.linalg.norm(W, axis=1, keepdims=True), 1e-12)
+    C = np.zeros((n_lab, W.shape[1]), np.float64)
+    np.add.at(C, labels[valid], W[valid])
+    C /= np.maximum(np.linalg.norm(C, axis=1, keepdims=True), 1e-12)
+    S = W[queries] @ C.T
+    own = S[np.arange(len(queries)), labels[queries]]
+    other = (S.sum(axis=1) - own) / (n_lab - 1)
+    return float((own - other).mean())
 
 
 def top_queries(counts: np.ndarray, labels: np.ndarray, n: int) -> np.ndarray:
