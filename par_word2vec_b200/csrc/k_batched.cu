@@ -739,12 +739,28 @@ struct LaneRow {
         }
         return r;
     }
-    // the lane's part of x . y with four independent partial sums (a chain of ceil(E/4) FMAs)
+    // The lane's part of x . y with four independent partial sums (element i into sum i mod 4, a
+    // chain of ceil(E/4) FMAs), formed two sums per instruction by the packed FP32 FMA of sm_100
+    // (each element rounds exactly as fmaf).
     __device__ static float dot(const float (&x)[E], const float (&y)[E]) {
-        float f[4] = {0.f, 0.f, 0.f, 0.f};
+        float2 f01 = make_float2(0.f, 0.f), f23 = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int i = 0; i < E; i++) f[i & 3] = fmaf(x[i], y[i], f[i & 3]);
-        return (f[0] + f[1]) + (f[2] + f[3]);
+        for (int k = 0; k < E; k += 2) {
+            const float2 p = make_float2(x[k], x[k + 1]), q = make_float2(y[k], y[k + 1]);
+            if (k & 2) f23 = __ffma2_rn(p, q, f23);
+            else f01 = __ffma2_rn(p, q, f01);
+        }
+        return (f01.x + f01.y) + (f23.x + f23.y);
+    }
+    // out = g * a + b, two elements per packed FMA (out may be b)
+    __device__ static void fma_scaled(float g, const float (&a)[E], const float (&b)[E], float (&out)[E]) {
+        const float2 g2 = make_float2(g, g);
+#pragma unroll
+        for (int k = 0; k < E; k += 2) {
+            const float2 r = __ffma2_rn(g2, make_float2(a[k], a[k + 1]), make_float2(b[k], b[k + 1]));
+            out[k] = r.x;
+            out[k + 1] = r.y;
+        }
     }
 };
 
@@ -884,15 +900,16 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                         T *x = w_in + (size_t) ctx_w[i] * ld;
                         float xv[E];
                         LR::widen(LR::load(x, lane, vm), xv);
-#pragma unroll
-                        for (int k = 0; k < E; k++) {
-                            dy[k] = fmaf(g, xv[k], dy[k]);
-                            xv[k] = fmaf(g, y[k], xv[k]);
-                        }
+                        LR::fma_scaled(g, xv, dy, dy);
+                        LR::fma_scaled(g, y, xv, xv);
                         if (g != 0.f) LR::store(x, LR::pack(xv, rb), lane, vm);
                     }
 #pragma unroll
-                    for (int k = 0; k < E; k++) y[k] += dy[k];
+                    for (int k = 0; k < E; k += 2) {
+                        const float2 r = __fadd2_rn(make_float2(y[k], y[k + 1]), make_float2(dy[k], dy[k + 1]));
+                        y[k] = r.x;
+                        y[k + 1] = r.y;
+                    }
                 } else if (n > 0) {
                     // contexts c in [lo_c, hi_c] without p, in window order; the first one and its
                     // row were read during the previous position (L > 1 gives every position one)
@@ -933,11 +950,8 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                             }
                             T *x = w_in + (size_t) word * ld;
                             float xw[E];
-#pragma unroll
-                            for (int k = 0; k < E; k++) {
-                                xw[k] = fmaf(g, y[k], xr[k]);
-                                y[k] = fmaf(g, xr[k], y[k]);
-                            }
+                            LR::fma_scaled(g, y, xr, xw);  // from the entry values of y
+                            LR::fma_scaled(g, xr, y, y);
                             const Raw r = LR::pack(xw, rb);
                             LR::store(x, r, lane, vm);
                             if (i + 2 < n || (BF16 && has_next && more)) {
@@ -976,11 +990,8 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                         f = warp_sum(f);
                         const float g = grad_from_table(f, 1, alpha, s_exp);
                         float xw[E];
-#pragma unroll
-                        for (int k = 0; k < E; k++) {
-                            xw[k] = fmaf(g, y[k], xr[k]);
-                            y[k] = fmaf(g, xr[k], y[k]);
-                        }
+                        LR::fma_scaled(g, y, xr, xw);  // from the entry values of y
+                        LR::fma_scaled(g, xr, y, y);
                         const Raw r = LR::pack(xw, rb);
                         LR::store(x, r, lane, vm);
                         if (ahead && wc == word) xn = r;
