@@ -87,6 +87,22 @@ def parse():
     return a
 
 
+TRAFFIC_PROFILES = {"batched_bf16": "k_stream_train_bf16_10M_tokens.md", "batched": "k_stream_train_fp32_10M_tokens.md",
+                    "plain": "k_plain_train_fp32_10M_tokens.md"}
+
+
+def measured_traffic_per_kept_position(mode: str):
+    """DRAM bytes per kept position of the training kernel, from the committed ncu summary of a
+    10M-token capture of the same kernel (the 800M-token launch is too large to capture)."""
+    import re
+    name = TRAFFIC_PROFILES.get(mode)
+    path = os.path.join(ROOT, "profiles", name) if name else None
+    if not path or not os.path.exists(path):
+        return None, None
+    m = re.search(r"traffic_bytes_per_kept_position:\s*([0-9.]+)", open(path).read())
+    return (float(m.group(1)), "profiles/" + name) if m else (None, None)
+
+
 def measured_peak_hbm():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -397,15 +413,17 @@ def main():
         peak, peak_src, bound = measured_l2_read_gbs(torch, dev), "measured here: L2 read bandwidth (32 MB buffer)", "l2"
     else:
         (peak, peak_src), bound = measured_peak_hbm(), "hbm"
+    tpp, tsrc = measured_traffic_per_kept_position(args.mode) if args.workload == "1b" else (None, None)
     roofline = {"bound": bound, "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "kernel": "training kernel", "peak_source": peak_src,
+                "traffic": tpp * kept if tpp else None, "kernel": "training kernel", "peak_source": peak_src,
                 "alg_bytes_per_launch": alg_bytes, "kernel_ms_per_launch": kernel_ms,
                 "pack_ms_per_launch": mean("pack_ms"), "alg_bytes_per_kept_position": alg_bytes / max(kept, 1),
                 "pair_bytes_per_kept_position": pair_bytes / max(kept, 1),
                 "pair_bytes_note": "B_pair = 2 s d (2 pairs + kept + negatives): every pair's two rows read and "
                                    "written, an upper bound on row traffic at the reference's granularity",
-                "traffic_note": "DRAM bytes of the same kernel from ncu are in profiles/ (captured on a smaller "
-                                "corpus, per kept position)"}
+                "traffic_note": (f"ncu dram__bytes_read+write per kept position of the same kernel ({tsrc}, a "
+                                 f"10M-token capture) x kept positions of this launch" if tpp else
+                                 "no ncu capture of this workload")}
 
     # ---- end to end through the C ABI with host buffers ----
     w_host = torch.empty((V, d), dtype=torch.float32, pin_memory=True).numpy()  # pinned, like the corpus
