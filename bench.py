@@ -79,6 +79,8 @@ def parse():
     ap.add_argument("--attraction", default="default", choices=["default", "sequential", "pipelined"],
                     help="attraction form (parw2v_config.attraction); pipelined = sequential up to rounding")
     ap.add_argument("--autotune", type=int, default=0, help="parw2v_config.autotune")
+    ap.add_argument("--variant", default="auto", choices=["auto", "stream", "window"],
+                    help="BATCHED kernel organisation (parw2v_config.variant); the result does not depend on it")
     ap.add_argument("--min-rounds", type=int, default=0,
                     help="parw2v_config.min_rounds (0: the library's cap on sentences in flight; -1: no cap, "
                          "as the 800M-token corpus runs uncapped under the default)")
@@ -388,7 +390,9 @@ def main():
                   "pipelined": pw.ATTRACT_PIPELINED}[args.attraction]
 
     def make(m, seed, min_rounds=None, stream=stream_np):
+        variant = {"auto": pw.VARIANT_AUTO, "stream": pw.VARIANT_STREAM, "window": pw.VARIANT_WINDOW}[args.variant]
         t = pw.Trainer(mode=m, device=local, seed=seed, staging=staging, attraction=attraction, autotune=args.autotune,
+                       variant=variant,
                        min_rounds=args.min_rounds if min_rounds is None else min_rounds, **hyper)
         t.set_vocab(counts)
         t.init_weights()
@@ -442,7 +446,8 @@ def main():
     cfg = static_config(args)
     cfg.update({"corpus_tokens_with_eos": n, "sentences": n_sent, "vocab_size": V, "min_rounds": args.min_rounds,
                 "staging": args.staging, "attraction": args.attraction, "autotune": args.autotune,
-                "replicas": world, "launch": {k: stats[0][k] for k in ("grid", "warps_per_cta", "lane_elems",
+                "variant": args.variant,
+                "replicas": world, "launch": {k: stats[0][k] for k in ("grid", "warps_per_cta", "variant", "lane_elems",
                                                                         "staging", "attraction", "repulsion")},
                 "l2": ("flushed before every step (256 MB write, outside the timed events); the tables fit in L2"
                        if l2_resident else "no flush: corpus (4 B/token) and weights exceed the 126 MB L2")})
@@ -495,6 +500,15 @@ def main():
     return 0
 
 
+def knob_kwargs(args, pw) -> dict:
+    """The launch knobs of this run (result-neutral), as Trainer keyword arguments."""
+    return dict(staging={"auto": pw.STAGING_AUTO, "bulk": pw.STAGING_BULK, "cpasync": pw.STAGING_CPASYNC}[args.staging],
+                attraction={"default": pw.ATTRACT_DEFAULT, "sequential": pw.ATTRACT_SEQUENTIAL,
+                            "pipelined": pw.ATTRACT_PIPELINED}[args.attraction],
+                variant={"auto": pw.VARIANT_AUTO, "stream": pw.VARIANT_STREAM, "window": pw.VARIANT_WINDOW}[args.variant],
+                autotune=args.autotune)
+
+
 def score_loss(pw, evaluate, counts, hyper, w_in, w_out, triples) -> float:
     with pw.Trainer(size=hyper["size"], mode=pw.MODE_PLAIN) as t:
         t.set_vocab(counts)
@@ -535,7 +549,7 @@ def reference_leg(args, pw, evaluate, hyper, dev, tmp, corpus_text, stream_np, c
     triples = evaluate.eval_triples(s2, c2, n_windows=4096, window=hyper["window"])
     queries = evaluate.top_queries(c2, l2, 10000)
     mode = pw.MODE_NAMES[args.mode]
-    with pw.Trainer(mode=mode, seed=1, min_rounds=ours_min_rounds, **hyper) as t:
+    with pw.Trainer(mode=mode, seed=1, min_rounds=ours_min_rounds, **knob_kwargs(args, pw), **hyper) as t:
         t.set_vocab(c2)
         t.init_weights()
         t.set_corpus(s2)

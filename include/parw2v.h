@@ -70,7 +70,8 @@ typedef struct {
                         shared memory */
     int autotune;    /* BATCHED modes: 1 = on the first parw2v_train (and whenever the number of
                         sentences in flight changes), time short trials of the launch knobs that
-                        do not change the result -- the split of the sentences in flight into CTAs
+                        do not change the result -- the kernel organisation (unless cfg.variant fixes
+                        it), the split of the sentences in flight into CTAs
                         and warps, the row elements per lane of the streamed kernel, the staging
                         copies (unless cfg.staging fixes them) and, with PARW2V_ATTRACT_DEFAULT, the
                         sequential attraction's plain or pipelined form -- on a prefix of the first epoch, with
@@ -122,6 +123,7 @@ typedef struct {
     int lane_elems;      /* BATCHED streamed kernel: row elements each lane holds */
     int staging;         /* BATCHED modes: PARW2V_STAGING_BULK or _CPASYNC as launched */
     int attraction;      /* PARW2V_ATTRACT_* form the training kernel ran */
+    int variant;         /* BATCHED modes: PARW2V_VARIANT_STREAM or _WINDOW as launched */
 } parw2v_stats;
 
 /* parw2v_stats.repulsion */

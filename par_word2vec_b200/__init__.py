@@ -61,7 +61,8 @@ class _Stats(ctypes.Structure):
                 ("pairs", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("negatives", ctypes.c_uint64),
                 ("kernel_ms", ctypes.c_double), ("pack_ms", ctypes.c_double), ("final_alpha", ctypes.c_float),
                 ("grid", ctypes.c_int), ("warps_per_cta", ctypes.c_int), ("repulsion", ctypes.c_int),
-                ("lane_elems", ctypes.c_int), ("staging", ctypes.c_int), ("attraction", ctypes.c_int)]
+                ("lane_elems", ctypes.c_int), ("staging", ctypes.c_int), ("attraction", ctypes.c_int),
+                ("variant", ctypes.c_int)]
 
 
 class _Trace(ctypes.Structure):

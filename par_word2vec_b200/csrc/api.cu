@@ -64,6 +64,7 @@ struct parw2v_ctx {
         bool done = false;
         uint64_t inflight = 0;
         int grid = 0, warps = 0, stage_bulk = 0, lane_elems = 0, attr_pipe = 0;
+        bool stream = true;
     } tuned;
 };
 
@@ -586,35 +587,45 @@ static uint64_t hogwild_cap(int min_rounds, uint64_t n_lines, uint64_t n_tokens)
 // every launch.  The fastest is kept in the context.  Returns an error only for a failed CUDA call;
 // without the memory for the weight backup it keeps the compiled-in choices.
 static int autotune(parw2v_ctx *c, TrainArgs a, int base_grid, int base_warps) {
-    const bool stream = stream_variant(c);
     const parw2v_config &k = c->cfg;
     c->tuned = {};
     struct Cand {
         int grid, warps, bulk, elems, pipe;
+        bool stream;
     };
-    std::vector<std::pair<int, int>> splits = {{base_grid, base_warps}};
-    for (int f : {2, 4})
-        if (base_warps % f == 0 &&
-            batched_ctas_per_sm(c->ld, k.window, k.negative, k.batch_size, c->bf16, stream, base_warps / f) >= f)
-            splits.push_back({base_grid * f, base_warps / f});
-    std::vector<int> elems = {0};
-    if (stream) {
-        const int e0 = stream_lane_elems_default(k.size), e1 = stream_lane_elems_next(e0);
-        elems = {e0};
-        if (e1) elems.push_back(e1);
-    }
     std::vector<int> bulks;
     if (k.staging != PARW2V_STAGING_AUTO) bulks = {k.staging == PARW2V_STAGING_BULK ? 1 : 0};
     else if (batched_tensor_repulsion(k.window, k.negative, k.batch_size)) bulks = {0, 1};
     else bulks = {0};
-    // the sequential attraction in its plain or pipelined form, unless cfg.attraction fixes one
-    std::vector<int> pipes = {a.attr_pipe};
-    if (stream && k.attraction == PARW2V_ATTRACT_DEFAULT) pipes = {0, 1};
     std::vector<Cand> cands;
-    for (auto &sp : splits)
-        for (int e : elems)
-            for (int b : bulks)
-                for (int pp : pipes) cands.push_back({sp.first, sp.second, b, e, pp});
+    // the kernel organisation: STREAM and, when the same sentences in flight fit its shared memory,
+    // WINDOW (both run the reference's order), unless cfg.variant fixes one
+    for (int v = 0; v < 2; v++) {
+        const bool stream = v == 0;
+        if ((stream && k.variant == PARW2V_VARIANT_WINDOW) || (!stream && k.variant == PARW2V_VARIANT_STREAM)) continue;
+        if (!stream && (k.attraction == PARW2V_ATTRACT_PIPELINED ||
+                        batched_max_warps(c->ld, k.window, k.negative, k.batch_size, c->bf16, nullptr, false) < base_warps))
+            continue;
+        std::vector<std::pair<int, int>> splits = {{base_grid, base_warps}};
+        for (int f : {2, 4})
+            if (base_warps % f == 0 &&
+                batched_ctas_per_sm(c->ld, k.window, k.negative, k.batch_size, c->bf16, stream, base_warps / f) >= f)
+                splits.push_back({base_grid * f, base_warps / f});
+        std::vector<int> elems = {0};
+        if (stream) {
+            const int e0 = stream_lane_elems_default(k.size), e1 = stream_lane_elems_next(e0);
+            elems = {e0};
+            if (e1) elems.push_back(e1);
+        }
+        // the sequential attraction in its plain or pipelined form, unless cfg.attraction fixes one
+        std::vector<int> pipes = {stream ? a.attr_pipe : 0};
+        if (stream && k.attraction == PARW2V_ATTRACT_DEFAULT) pipes = {0, 1};
+        for (auto &sp : splits)
+            for (int e : elems)
+                for (int b : bulks)
+                    for (int pp : pipes) cands.push_back({sp.first, sp.second, b, e, pp, stream});
+    }
+    if (cands.empty()) return PARW2V_OK;
     // epoch 0's packed corpus
     CK(c, cudaMemsetAsync(&c->d_cnt->work, 0, sizeof(unsigned long long), c->stream), "autotune");
     CK(c, launch_pack(a, c->d_packed, c->d_line_end, c->d_tile_kept, c->d_tile_zero, pack_tiles(c->n_tokens), c->stream),
@@ -653,7 +664,7 @@ static int autotune(parw2v_ctx *c, TrainArgs a, int base_grid, int base_warps) {
             hc.work = 0;
             e = cudaMemcpyAsync(c->d_cnt, &hc, sizeof(hc), cudaMemcpyHostToDevice, c->stream);
             if (e == cudaSuccess) e = cudaEventRecord(c->ev0, c->stream);
-            if (e == cudaSuccess) e = launch_batched_train(a, c->bf16, stream, cd.grid, cd.warps, c->stream);
+            if (e == cudaSuccess) e = launch_batched_train(a, c->bf16, cd.stream, cd.grid, cd.warps, c->stream);
             if (e == cudaSuccess) e = cudaEventRecord(c->ev1, c->stream);
             if (e == cudaSuccess) e = copy(c->d_w_in, backup);
             if (e == cudaSuccess) e = copy(c->d_w_out, (char *) backup + wbytes);
@@ -661,9 +672,10 @@ static int autotune(parw2v_ctx *c, TrainArgs a, int base_grid, int base_warps) {
             if (e == cudaSuccess && pass == 1) e = cudaEventElapsedTime(&ms, c->ev0, c->ev1);
         }
         if (e == cudaSuccess && log_trials)
-            fprintf(stderr, "parw2v autotune: grid %d x %d warps, %d elements per lane, staging %s, attraction %s: "
+            fprintf(stderr, "parw2v autotune: %s, grid %d x %d warps, %d elements per lane, staging %s, attraction %s: "
                             "%.3f ms for %llu lines\n",
-                    cd.grid, cd.warps, cd.elems ? cd.elems : stream_lane_elems_default(k.size),
+                    cd.stream ? "stream" : "window", cd.grid, cd.warps,
+                    cd.stream ? (cd.elems ? cd.elems : stream_lane_elems_default(k.size)) : 0,
                     cd.bulk ? "bulk" : "cp.async", cd.pipe ? "pipelined" : "sequential", ms,
                     (unsigned long long) trial);
         if (e == cudaSuccess && (i == 0 || ms < best_ms)) {
@@ -682,6 +694,7 @@ static int autotune(parw2v_ctx *c, TrainArgs a, int base_grid, int base_warps) {
     c->tuned.stage_bulk = best.bulk;
     c->tuned.lane_elems = best.elems;
     c->tuned.attr_pipe = best.pipe;
+    c->tuned.stream = best.stream;
     return PARW2V_OK;
 }
 
@@ -692,6 +705,7 @@ static int train_hogwild(parw2v_ctx *c, TrainArgs &a, parw2v_stats *st) {
     int grid = c->cfg.grid;
     int warps = c->cfg.warps_per_cta;
     const bool plain = c->cfg.mode == PARW2V_MODE_PLAIN;
+    bool stream = stream_variant(c);  // BATCHED kernel organisation (the autotuner may change it)
     if (plain) {
         warps = plain_warps_per_cta(warps);
         if (!grid) grid = sms * 2;
@@ -735,6 +749,7 @@ static int train_hogwild(parw2v_ctx *c, TrainArgs &a, parw2v_stats *st) {
             a.stage_bulk = c->tuned.stage_bulk;
             a.lane_elems = c->tuned.lane_elems;
             a.attr_pipe = c->tuned.attr_pipe;
+            stream = c->tuned.stream;
         }
     }
     c->last_grid = grid;
@@ -760,7 +775,7 @@ static int train_hogwild(parw2v_ctx *c, TrainArgs &a, parw2v_stats *st) {
                                 c->stream);
         } else {
             e = plain ? launch_plain_train(a, grid, warps, c->stream)
-                      : launch_batched_train(a, c->bf16, stream_variant(c), grid, warps, c->stream);
+                      : launch_batched_train(a, c->bf16, stream, grid, warps, c->stream);
             if (e == cudaSuccess) e = launch_advance_epoch(c->d_cnt, c->stream);
         }
         const cudaError_t ec = cudaStreamEndCapture(c->stream, &graph);
@@ -814,7 +829,8 @@ static int train_hogwild(parw2v_ctx *c, TrainArgs &a, parw2v_stats *st) {
         st->final_alpha = std::max(end_alpha, c->cfg.alpha * 0.0001f);
         st->grid = grid;
         st->warps_per_cta = warps;
-        st->lane_elems = plain ? 0 : (a.lane_elems ? a.lane_elems : (stream_variant(c) ? stream_lane_elems_default(c->cfg.size) : 0));
+        st->lane_elems = plain || !stream ? 0 : (a.lane_elems ? a.lane_elems : stream_lane_elems_default(c->cfg.size));
+        st->variant = plain ? 0 : (stream ? PARW2V_VARIANT_STREAM : PARW2V_VARIANT_WINDOW);
         st->staging = plain ? 0 : (a.stage_bulk ? PARW2V_STAGING_BULK : PARW2V_STAGING_CPASYNC);
         st->attraction = a.sync_window ? PARW2V_ATTRACT_WINDOW
                                        : (!plain && a.attr_pipe ? PARW2V_ATTRACT_PIPELINED : PARW2V_ATTRACT_SEQUENTIAL);
