@@ -118,11 +118,13 @@ __device__ __forceinline__ bool stage_rows(Stager &st, const T *w_in, const T *w
         st.phase ^= 1u;
     } else {
         const unsigned pieces = bytes / 16u;
-        // row of piece `it`: it / pieces by a multiply-high (exact for it < 128 * pieces; a row is
-        // at least 32 bytes, so pieces >= 2)
+        // row of piece `it`: a shift for the 2 or 4 pieces of a column chunk, else it / pieces by a
+        // multiply-high (exact for it < 128 * pieces; a row is at least 32 bytes, so pieces >= 2)
+        const int shift = pieces == 4u ? 2 : (pieces == 2u ? 1 : -1);
         const unsigned inv = 0xFFFFFFFFu / pieces + 1u;
         for (unsigned it = lane; it < (unsigned) (rows + nk) * pieces; it += 32) {
-            const int r = (int) __umulhi(it, inv), pc = (int) (it - (unsigned) r * pieces);
+            const int r = shift >= 0 ? (int) (it >> shift) : (int) __umulhi(it, inv);
+            const int pc = (int) (it - (unsigned) r * pieces);
             const T *src = r < rows ? w_in + (size_t) sbw[r] * ld : w_out + (size_t) negs[r - rows] * ld;
             T *dst = r < rows ? sin + (size_t) r * stride : sout + (size_t) (r - rows) * stride;
             const unsigned s = smem_u32(reinterpret_cast<unsigned char *>(dst) + 16 * pc);
@@ -354,11 +356,12 @@ __device__ __noinline__ bool repel_bf16(const TrainArgs &a, const Geom &geo, uns
                 unsigned af[4];
                 ldsm_x4_t(af, sout + (size_t) (16 * ks + a_row) * S + c + a_col);
 #pragma unroll
-                for (int nt = 0; nt < 4; nt++)
-                    if (nt < ntq) {
-                        unsigned b[2];
-                        ldsm_x2_t(b, Gb + (size_t) (16 * ks + (lane & 15)) * kGbStride + 8 * nt);
-                        mma16816(q[nt], af, b[0], b[1]);
+                for (int np = 0; np < 2; np++)
+                    if (2 * np < ntq) {
+                        unsigned b[4];  // G rows 16ks..16ks+15 at columns 16np..16np+15: n-tiles 2np, 2np+1
+                        ldsm_x4_t(b, Gb + (size_t) (16 * ks + (lane & 15)) * kGbStride + 16 * np + ((lane >> 4) << 3));
+                        mma16816(q[2 * np], af, b[0], b[1]);
+                        if (2 * np + 1 < ntq) mma16816(q[2 * np + 1], af, b[2], b[3]);
                     }
             }
 #pragma unroll
