@@ -74,7 +74,7 @@ def parse():
     ap.add_argument("--tokens", type=int, default=None, help="1b workload: corpus tokens (without </s>)")
     ap.add_argument("--no-compare", action="store_true", help="skip the other modes and the quality scores")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the reference CPU leg")
-    ap.add_argument("--staging", default="auto", choices=["auto", "bulk", "cpasync", "rows"],
+    ap.add_argument("--staging", default="auto", choices=["auto", "bulk", "cpasync"],
                     help="repulsion staging copies (parw2v_config.staging); the result does not depend on it")
     ap.add_argument("--attraction", default="default", choices=["default", "sequential", "pipelined"],
                     help="attraction form (parw2v_config.attraction); pipelined = sequential up to rounding")
@@ -379,8 +379,7 @@ def main():
     V = len(counts)
     mode = pw.MODE_NAMES[args.mode]
     bytes_per = 2 if mode == pw.MODE_BATCHED_BF16 else 4
-    staging = {"auto": pw.STAGING_AUTO, "bulk": pw.STAGING_BULK, "cpasync": pw.STAGING_CPASYNC,
-               "rows": pw.STAGING_ROWS}[args.staging]
+    staging = {"auto": pw.STAGING_AUTO, "bulk": pw.STAGING_BULK, "cpasync": pw.STAGING_CPASYNC}[args.staging]
     l2_resident = args.workload != "1b"
     flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device=dev) if l2_resident else None
 
@@ -503,8 +502,7 @@ def main():
 
 def knob_kwargs(args, pw) -> dict:
     """The launch knobs of this run (result-neutral), as Trainer keyword arguments."""
-    return dict(staging={"auto": pw.STAGING_AUTO, "bulk": pw.STAGING_BULK, "cpasync": pw.STAGING_CPASYNC,
-                         "rows": pw.STAGING_ROWS}[args.staging],
+    return dict(staging={"auto": pw.STAGING_AUTO, "bulk": pw.STAGING_BULK, "cpasync": pw.STAGING_CPASYNC}[args.staging],
                 attraction={"default": pw.ATTRACT_DEFAULT, "sequential": pw.ATTRACT_SEQUENTIAL,
                             "pipelined": pw.ATTRACT_PIPELINED}[args.attraction],
                 variant={"auto": pw.VARIANT_AUTO, "stream": pw.VARIANT_STREAM, "window": pw.VARIANT_WINDOW}[args.variant],

@@ -81,15 +81,11 @@ typedef struct {
 } parw2v_config;
 
 /* Repulsion staging of the BATCHED modes (cfg.staging); the result does not depend on it */
-#define PARW2V_STAGING_AUTO 0     /* CPASYNC; ROWS when a CTA runs at most 4 warps (the number
-                                     in flight is capped) and the whole rows fit */
+#define PARW2V_STAGING_AUTO 0     /* CPASYNC (measured faster for these 64-byte row chunks) */
 #define PARW2V_STAGING_BULK 1     /* one bulk copy (cp.async.bulk, the TMA unit) per row and column
                                      chunk, completing on a shared-memory mbarrier, and one bulk
                                      store per row and chunk for the BF16 write-back */
-#define PARW2V_STAGING_CPASYNC 2  /* 16-byte cp.async copies and 16-byte stores, 64-byte column
-                                     chunks (one wait per chunk and pass) */
-#define PARW2V_STAGING_ROWS 3     /* 16-byte cp.async copies of whole rows (one wait per pass), where
-                                     shared memory holds them; else CPASYNC */
+#define PARW2V_STAGING_CPASYNC 2  /* 16-byte cp.async copies and 16-byte stores */
 
 /* Kernel organisation of the BATCHED modes (cfg.variant) */
 #define PARW2V_VARIANT_AUTO 0    /* STREAM */

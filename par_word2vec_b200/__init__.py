@@ -25,7 +25,7 @@ EXP_TABLE_SIZE = 1000
 
 ATTRACT_DEFAULT, ATTRACT_SEQUENTIAL, ATTRACT_WINDOW, ATTRACT_PIPELINED = 0, 1, 2, 3
 VARIANT_AUTO, VARIANT_WINDOW, VARIANT_STREAM = 0, 1, 2
-STAGING_AUTO, STAGING_BULK, STAGING_CPASYNC, STAGING_ROWS = 0, 1, 2, 3
+STAGING_AUTO, STAGING_BULK, STAGING_CPASYNC = 0, 1, 2
 REPULSION_SERIAL, REPULSION_TENSOR, REPULSION_CUDA = 0, 1, 2
 OK, ERR_ARG, ERR_CUDA, ERR_OOM, ERR_CAPACITY, ERR_TIMEOUT, ERR_STATE, ERR_IO, ERR_NODEV = 0, -1, -2, -3, -4, -5, -6, -7, -8
 

@@ -63,7 +63,7 @@ struct parw2v_ctx {
     struct {
         bool done = false;
         uint64_t inflight = 0;
-        int grid = 0, warps = 0, stage_bulk = 0, lane_elems = 0, attr_pipe = 0, rep_wide = 0;
+        int grid = 0, warps = 0, stage_bulk = 0, lane_elems = 0, attr_pipe = 0;
         bool stream = true;
     } tuned;
 };
@@ -173,7 +173,7 @@ int parw2v_create(const parw2v_config *cfg, parw2v_ctx **out) {
         return fail(nullptr, PARW2V_ERR_ARG, "invalid kernel variant");
     if (k.attraction < PARW2V_ATTRACT_DEFAULT || k.attraction > PARW2V_ATTRACT_PIPELINED)
         return fail(nullptr, PARW2V_ERR_ARG, "invalid attraction variant");
-    if (k.staging < PARW2V_STAGING_AUTO || k.staging > PARW2V_STAGING_ROWS)
+    if (k.staging < PARW2V_STAGING_AUTO || k.staging > PARW2V_STAGING_CPASYNC)
         return fail(nullptr, PARW2V_ERR_ARG, "invalid staging method");
     if (k.window > 100 || k.negative > 100 || k.batch_size > 1000)
         return fail(nullptr, PARW2V_ERR_CAPACITY, "window/negative/batch_size beyond the supported range");
@@ -580,13 +580,6 @@ static uint64_t hogwild_cap(int min_rounds, uint64_t n_lines, uint64_t n_tokens)
     return std::max<uint64_t>(std::max<uint64_t>(1, 7000 / per_line), n_lines / 8192);
 }
 
-// Whole-row repulsion staging fits `warps` warps per CTA of the given organisation.
-static bool rows_staging_fits(const parw2v_ctx *c, bool stream, int warps) {
-    const parw2v_config &k = c->cfg;
-    return batched_tensor_repulsion(k.window, k.negative, k.batch_size) &&
-           batched_max_warps(c->ld, k.window, k.negative, k.batch_size, c->bf16, nullptr, stream, true) >= warps;
-}
-
 // The autotuner (cfg.autotune): short timed trials of the BATCHED launch knobs that leave the
 // result unchanged -- how the sentences in flight split into CTAs and warps (their number stays),
 // the row elements per lane of the streamed kernel, the staging copies -- each on a prefix of the
@@ -599,14 +592,10 @@ static int autotune(parw2v_ctx *c, TrainArgs a, int base_grid, int base_warps) {
     struct Cand {
         int grid, warps, bulk, elems, pipe;
         bool stream;
-        int wide;
     };
-    // staging: 0 cp.async chunks, 1 bulk chunks, 2 cp.async whole rows (where they fit)
     std::vector<int> bulks;
-    if (k.staging == PARW2V_STAGING_BULK) bulks = {1};
-    else if (k.staging == PARW2V_STAGING_CPASYNC) bulks = {0};
-    else if (k.staging == PARW2V_STAGING_ROWS) bulks = {2};
-    else if (batched_tensor_repulsion(k.window, k.negative, k.batch_size)) bulks = {0, 1, 2};
+    if (k.staging != PARW2V_STAGING_AUTO) bulks = {k.staging == PARW2V_STAGING_BULK ? 1 : 0};
+    else if (batched_tensor_repulsion(k.window, k.negative, k.batch_size)) bulks = {0, 1};
     else bulks = {0};
     std::vector<Cand> cands;
     // the kernel organisation: STREAM and, when the same sentences in flight fit its shared memory,
@@ -633,10 +622,8 @@ static int autotune(parw2v_ctx *c, TrainArgs a, int base_grid, int base_warps) {
         if (stream && k.attraction == PARW2V_ATTRACT_DEFAULT) pipes = {0, 1};
         for (auto &sp : splits)
             for (int e : elems)
-                for (int b : bulks) {
-                    if (b == 2 && !rows_staging_fits(c, stream, sp.second)) continue;
-                    for (int pp : pipes) cands.push_back({sp.first, sp.second, b == 1, e, pp, stream, b == 2});
-                }
+                for (int b : bulks)
+                    for (int pp : pipes) cands.push_back({sp.first, sp.second, b, e, pp, stream});
     }
     if (cands.empty()) return PARW2V_OK;
     // epoch 0's packed corpus
@@ -670,7 +657,6 @@ static int autotune(parw2v_ctx *c, TrainArgs a, int base_grid, int base_warps) {
         a.stage_bulk = cd.bulk;
         a.lane_elems = cd.elems;
         a.attr_pipe = cd.pipe;
-        a.rep_wide = cd.wide;
         float ms = 0.f;
         for (int pass = 0; pass < 2 && e == cudaSuccess; pass++) {
             DevCounters hc = h0;
@@ -690,7 +676,7 @@ static int autotune(parw2v_ctx *c, TrainArgs a, int base_grid, int base_warps) {
                             "%.3f ms for %llu lines\n",
                     cd.stream ? "stream" : "window", cd.grid, cd.warps,
                     cd.stream ? (cd.elems ? cd.elems : stream_lane_elems_default(k.size)) : 0,
-                    cd.bulk ? "bulk" : (cd.wide ? "cp.async rows" : "cp.async"), cd.pipe ? "pipelined" : "sequential", ms,
+                    cd.bulk ? "bulk" : "cp.async", cd.pipe ? "pipelined" : "sequential", ms,
                     (unsigned long long) trial);
         if (e == cudaSuccess && (i == 0 || ms < best_ms)) {
             best_ms = ms;
@@ -709,7 +695,6 @@ static int autotune(parw2v_ctx *c, TrainArgs a, int base_grid, int base_warps) {
     c->tuned.lane_elems = best.elems;
     c->tuned.attr_pipe = best.pipe;
     c->tuned.stream = best.stream;
-    c->tuned.rep_wide = best.wide;
     return PARW2V_OK;
 }
 
@@ -753,9 +738,6 @@ static int train_hogwild(parw2v_ctx *c, TrainArgs &a, parw2v_stats *st) {
             grid = (int) std::min<uint64_t>((uint64_t) std::min(grid, sms), std::max<uint64_t>(1, cap / (uint64_t) warps));
         }
     }
-    // whole-row staging: asked for, or by default when few warps per CTA leave shared memory free
-    if (!plain && (c->cfg.staging == PARW2V_STAGING_ROWS || (c->cfg.staging == PARW2V_STAGING_AUTO && warps <= 4)))
-        a.rep_wide = rows_staging_fits(c, stream, warps) ? 1 : 0;
     if (!plain && c->cfg.autotune) {
         const uint64_t inflight = (uint64_t) grid * warps;
         if (!c->tuned.done || c->tuned.inflight != inflight) {
@@ -767,7 +749,6 @@ static int train_hogwild(parw2v_ctx *c, TrainArgs &a, parw2v_stats *st) {
             a.stage_bulk = c->tuned.stage_bulk;
             a.lane_elems = c->tuned.lane_elems;
             a.attr_pipe = c->tuned.attr_pipe;
-            a.rep_wide = c->tuned.rep_wide;
             stream = c->tuned.stream;
         }
     }
@@ -850,7 +831,7 @@ static int train_hogwild(parw2v_ctx *c, TrainArgs &a, parw2v_stats *st) {
         st->warps_per_cta = warps;
         st->lane_elems = plain || !stream ? 0 : (a.lane_elems ? a.lane_elems : stream_lane_elems_default(c->cfg.size));
         st->variant = plain ? 0 : (stream ? PARW2V_VARIANT_STREAM : PARW2V_VARIANT_WINDOW);
-        st->staging = plain ? 0 : (a.stage_bulk ? PARW2V_STAGING_BULK : (a.rep_wide ? PARW2V_STAGING_ROWS : PARW2V_STAGING_CPASYNC));
+        st->staging = plain ? 0 : (a.stage_bulk ? PARW2V_STAGING_BULK : PARW2V_STAGING_CPASYNC);
         st->attraction = a.sync_window ? PARW2V_ATTRACT_WINDOW
                                        : (!plain && a.attr_pipe ? PARW2V_ATTRACT_PIPELINED : PARW2V_ATTRACT_SEQUENTIAL);
         st->repulsion = plain ? PARW2V_REPULSION_SERIAL

@@ -58,7 +58,6 @@ struct TrainArgs {
     int stage_bulk;          // BATCHED repulsion staging: 1 bulk copies (TMA unit), 0 16-byte cp.async
     int lane_elems;          // streamed kernel: row elements per lane (0 = the smallest that holds d)
     int attr_pipe;           // streamed kernel: sequential attraction in its pipelined form
-    int rep_wide;            // BATCHED repulsion: stage whole rows at once (few warps per SM)
 };
 
 // Launchers (return a cudaError_t)
@@ -78,13 +77,11 @@ cudaError_t launch_plain_train(const TrainArgs &a, int grid, int warps_per_cta, 
 cudaError_t launch_batched_train(const TrainArgs &a, bool bf16, bool stream, int grid, int warps_per_cta, cudaStream_t s);
 size_t plain_scratch_floats(int ld, int batch, int window, int negative);
 int plain_warps_per_cta(int requested);
-int batched_max_warps(int ld, int window, int negative, int batch, bool bf16, size_t *smem_per_warp, bool stream,
-                      bool wide = false);
+int batched_max_warps(int ld, int window, int negative, int batch, bool bf16, size_t *smem_per_warp, bool stream);
 bool batched_tensor_repulsion(int window, int negative, int batch);  // the BATCHED modes' repulsion path
 // CTAs of `warps` warps of the BATCHED kernel that fit on one SM at once (shared memory, threads,
 // registers at the kernel's 128-register bound)
-int batched_ctas_per_sm(int ld, int window, int negative, int batch, bool bf16, bool stream, int warps,
-                       bool wide = false);
+int batched_ctas_per_sm(int ld, int window, int negative, int batch, bool bf16, bool stream, int warps);
 // the streamed kernel's row elements per lane: the default for d, and the next larger one (0 if none)
 int stream_lane_elems_default(int d);
 int stream_lane_elems_next(int e);

@@ -65,7 +65,7 @@ constexpr size_t kSmemHead = kExpBytes + 32;
 static_assert(sizeof(FastMod) == 16, "the 2w divisor takes 16 of the 32 bytes");
 static_assert(kExpBytes % 16 == 0, "the constants after the expTable are 16-byte aligned");
 
-__host__ __device__ inline Layout make_layout(int ld, int window, int negative, int batch, bool bf16, bool wide = false) {
+__host__ __device__ inline Layout make_layout(int ld, int window, int negative, int batch, bool bf16) {
     Layout L;
     L.ws = 2 * window + 1 + kPrefetch;
     L.kmax = 2 * window * negative;
@@ -80,7 +80,7 @@ __host__ __device__ inline Layout make_layout(int ld, int window, int negative, 
     if (ch > ((ld + 3) / 4) * 4) ch = ((ld + 3) / 4) * 4;
     if (ch < 16) ch = 16;
     L.ch = (int) ch;
-    L.geo = rep::make_geom(window, negative, batch, bf16, wide, ld);
+    L.geo = rep::make_geom(window, negative, batch, bf16);
     const size_t rep_bytes = L.geo.mma ? L.geo.bytes : up16(rows_rep * (size_t) (L.ch + 4) * 4);
     L.region = win_total > rep_bytes ? win_total : rep_bytes;
     L.tgt_off = L.region;
@@ -293,7 +293,7 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
     const int w = a.window, B = a.batch, ld = a.ld, d = a.d;
     const FastMod mod_w((uint32_t) w), mod_2w((uint32_t) (2 * w));
     const int n4 = (d + 3) >> 2;  // float4 chunks that carry data (the padding stays zero)
-    const Layout Lo = make_layout(ld, w, a.negative, B, BF16, a.rep_wide);
+    const Layout Lo = make_layout(ld, w, a.negative, B, BF16);
     float *s_exp = reinterpret_cast<float *>(smem_raw);
     for (int i = threadIdx.x; i <= kExpTableSize; i += blockDim.x) s_exp[i] = a.exp_table[i];
     __syncthreads();
@@ -591,7 +591,7 @@ __global__ void __launch_bounds__(kMaxWarpsB * 32, 1) k_batched_train(TrainArgs 
 
 template <int NV4, bool BF16, bool SYNC>
 cudaError_t launch_nvs(const TrainArgs &a, int grid, int warps, cudaStream_t s) {
-    const Layout Lo = make_layout(a.ld, a.window, a.negative, a.batch, BF16, a.rep_wide);
+    const Layout Lo = make_layout(a.ld, a.window, a.negative, a.batch, BF16);
     const size_t smem = kSmemHead + (size_t) warps * Lo.per_warp;
     cudaError_t e = cudaFuncSetAttribute(k_batched_train<NV4, BF16, SYNC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int) smem);
@@ -615,12 +615,11 @@ constexpr int kMaxWarpsS = 16;
 constexpr int kStreamStats = 5;  // kept, sentences, pairs, batches, negatives (per warp, in shared memory)
 constexpr size_t kSimtStage = 6400;  // CUDA-core repulsion staging bytes (column chunk as wide as fits)
 
-__host__ __device__ inline Layout make_layout_stream(int ld, int window, int negative, int batch, bool bf16,
-                                                     bool wide = false) {
+__host__ __device__ inline Layout make_layout_stream(int ld, int window, int negative, int batch, bool bf16) {
     Layout L;
     L.ws = 0;
     L.kmax = 2 * window * negative;
-    L.geo = rep::make_geom(window, negative, batch, bf16, wide, ld);
+    L.geo = rep::make_geom(window, negative, batch, bf16);
     L.raw_off = 0;
     L.tgt_off = 0;
     L.meta_off = 0;
@@ -778,7 +777,7 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int w = a.window, B = a.batch, ld = a.ld;
     const FastMod mod_w((uint32_t) w);
-    const Layout Lo = make_layout_stream(ld, w, a.negative, B, BF16, a.rep_wide);
+    const Layout Lo = make_layout_stream(ld, w, a.negative, B, BF16);
     float *s_exp = reinterpret_cast<float *>(smem_raw);
     FastMod *s_mod_2w = reinterpret_cast<FastMod *>(smem_raw + kExpBytes);
     uint64_t *s_totals = reinterpret_cast<uint64_t *>(smem_raw + kExpBytes + sizeof(FastMod));  // lines, kept
@@ -1050,7 +1049,7 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
 
 template <bool BF16, int E, int ATT>
 cudaError_t launch_stream_e(const TrainArgs &a, int grid, int warps, cudaStream_t s) {
-    const Layout Lo = make_layout_stream(a.ld, a.window, a.negative, a.batch, BF16, a.rep_wide);
+    const Layout Lo = make_layout_stream(a.ld, a.window, a.negative, a.batch, BF16);
     const size_t smem = kSmemHead + (size_t) warps * Lo.per_warp;
     cudaError_t e = cudaFuncSetAttribute(k_stream_train<BF16, E, ATT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
     if (e != cudaSuccess) return e;
@@ -1095,9 +1094,8 @@ cudaError_t launch_mode(const TrainArgs &a, int grid, int warps, cudaStream_t s)
 
 }  // namespace
 
-int batched_max_warps(int ld, int window, int negative, int batch, bool bf16, size_t *per_warp, bool stream, bool wide) {
-    const Layout Lo = stream ? make_layout_stream(ld, window, negative, batch, bf16, wide)
-                             : make_layout(ld, window, negative, batch, bf16, wide);
+int batched_max_warps(int ld, int window, int negative, int batch, bool bf16, size_t *per_warp, bool stream) {
+    const Layout Lo = stream ? make_layout_stream(ld, window, negative, batch, bf16) : make_layout(ld, window, negative, batch, bf16);
     if (per_warp) *per_warp = Lo.per_warp;
     const size_t avail = kSmemBudget - kSmemHead;
     long w = (long) (avail / Lo.per_warp);
@@ -1106,9 +1104,8 @@ int batched_max_warps(int ld, int window, int negative, int batch, bool bf16, si
     return (int) w;
 }
 
-int batched_ctas_per_sm(int ld, int window, int negative, int batch, bool bf16, bool stream, int warps, bool wide) {
-    const Layout Lo = stream ? make_layout_stream(ld, window, negative, batch, bf16, wide)
-                             : make_layout(ld, window, negative, batch, bf16, wide);
+int batched_ctas_per_sm(int ld, int window, int negative, int batch, bool bf16, bool stream, int warps) {
+    const Layout Lo = stream ? make_layout_stream(ld, window, negative, batch, bf16) : make_layout(ld, window, negative, batch, bf16);
     const size_t smem = kSmemHead + (size_t) warps * Lo.per_warp + 1024;  // + the CTA's reserved 1 KB
     const int by_smem = (int) ((228u * 1024u) / smem);
     const int by_threads = 2048 / (32 * warps);

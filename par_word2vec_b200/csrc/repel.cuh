@@ -30,10 +30,13 @@ namespace rep {
 constexpr int kRows = 32;       // batch rows on the tensor-core paths (staging rows of M_in)
 constexpr int kSweepNeg = 48;   // negatives per pass-1 sweep (3 m-tiles of accumulators)
 constexpr int kMaxMt = 6;       // m-tiles of negatives: K <= 96 on the tensor-core paths
-constexpr int kCols = 32;       // BF16 columns per chunk (64 B per row; 80-byte staged rows)
+constexpr int kStride = 40;     // staged row stride in BF16 (80 B: conflict-free ldmatrix rows)
+constexpr int kCols = 32;       // BF16 columns per chunk (64 B per row)
 constexpr int kF32Cols = 16;    // FP32 columns per chunk (the same 64 B per row)
+constexpr int kF32Stride = 20;  // staged FP32 row stride in floats (80 B)
 constexpr int kGbStride = 40;   // BF16 G row stride (80 B)
 constexpr int kGps = 36;        // FP32 G row stride in floats (144 B: conflict-free ldmatrix rows)
+static_assert(kF32Stride * 4 == kStride * 2, "FP32 and BF16 staging rows take the same bytes");
 
 __host__ __device__ constexpr size_t up16(size_t x) { return (x + 15) & ~(size_t) 15; }
 
@@ -43,29 +46,19 @@ struct Geom {
     int kcap;       // negatives a batch can draw: rep_b * negative with rep_b < 2 * window
     int mt;         // m-tiles of negatives: ceil(kcap / 16)
     bool mma;       // tensor-core path (rows <= kRows, kcap <= 16 * kMaxMt)
-    int cols;       // columns staged at a time: a 64-byte chunk, or (wide) the whole row of ld
-    int stride;     // staged row stride in elements: cols + 16 bytes, an odd number of 16-byte
-                    // units, so the 8 rows an ldmatrix reads fall in distinct shared-memory banks
-    size_t stage;   // staging: kRows batch rows, then 16 * mt negative rows, `stride` elements each
+    size_t stage;   // staging: kRows batch rows, then 16 * mt negative rows, 80 B each
     size_t gb;      // G kept through pass 2: BF16 16*mt x kGbStride, or FP32 16*mt x kGps
     size_t gf;      // FP32 G, kcap x kRows, for the table lookup and merging (may alias the staging)
     size_t bytes;   // region size
 };
 
-// wide: stage whole rows (ld columns, a multiple of 16 BF16 / 8 FP32 elements) at once, so a batch
-// waits for its copies twice (once per pass) instead of once per 64-byte column chunk: for few warps
-// per SM, where nothing hides those waits and shared memory is plentiful.
-__host__ __device__ inline Geom make_geom(int window, int negative, int batch, bool bf16, bool wide = false,
-                                          int ld = 0) {
+__host__ __device__ inline Geom make_geom(int window, int negative, int batch, bool bf16) {
     Geom g{};
     g.kcap = (2 * window - 1) * negative;
     g.mt = (g.kcap + 15) / 16;
     g.mma = batch <= kRows && g.kcap <= 16 * kMaxMt;
     if (!g.mma) return g;
-    const int esz = bf16 ? 2 : 4;
-    g.cols = wide && ld > 0 ? ld : (bf16 ? kCols : kF32Cols);
-    g.stride = g.cols + 16 / esz;
-    const size_t stage_bytes = up16((size_t) (kRows + 16 * g.mt) * g.stride * esz);
+    const size_t stage_bytes = up16((size_t) (kRows + 16 * g.mt) * kStride * 2);
     const size_t gf_bytes = up16((size_t) g.kcap * kRows * 4);
     const size_t gb_bytes = bf16 ? up16((size_t) 16 * g.mt * kGbStride * 2) : up16((size_t) 16 * g.mt * kGps * 4);
     g.stage = 0;
@@ -91,7 +84,7 @@ struct Stager {
 };
 
 // Stage columns [col0, col0 + ncols) of the batch rows (words sbw[0..rows)) into `sin` and of the
-// negatives negs[0..nk) into `sout` (row stride `stride` elements).  ncols * esz is a multiple
+// negatives negs[0..nk) into `sout` (row stride kStride BF16 = 80 B).  ncols * esz is a multiple
 // of 16 bytes.  Returns false (warp-uniform) if a bulk copy did not complete in time.
 template <typename T>
 __device__ __forceinline__ bool stage_rows(Stager &st, const T *w_in, const T *w_out, int ld, int col0, int ncols,
@@ -117,14 +110,10 @@ __device__ __forceinline__ bool stage_rows(Stager &st, const T *w_in, const T *w
         if (!ok) mbar_wait_bounded(st.bar, st.phase, kMaxBulkPolls);
         st.phase ^= 1u;
     } else {
-        const unsigned pieces = bytes / 16u;
-        // row of piece `it`: a shift for the 2 or 4 pieces of a column chunk, else it / pieces by a
-        // multiply-high (exact for it < 128 * pieces; a row is at least 32 bytes, so pieces >= 2)
-        const int shift = pieces == 4u ? 2 : (pieces == 2u ? 1 : -1);
-        const unsigned inv = 0xFFFFFFFFu / pieces + 1u;
-        for (unsigned it = lane; it < (unsigned) (rows + nk) * pieces; it += 32) {
-            const int r = shift >= 0 ? (int) (it >> shift) : (int) __umulhi(it, inv);
-            const int pc = (int) (it - (unsigned) r * pieces);
+        const int pieces = (int) (bytes / 16);
+        const int shift = pieces == 4 ? 2 : (pieces == 2 ? 1 : 0);  // pieces per row: 1, 2 or 4
+        for (int it = lane; it < (rows + nk) << shift; it += 32) {
+            const int r = it >> shift, pc = it & (pieces - 1);
             const T *src = r < rows ? w_in + (size_t) sbw[r] * ld : w_out + (size_t) negs[r - rows] * ld;
             T *dst = r < rows ? sin + (size_t) r * stride : sout + (size_t) (r - rows) * stride;
             const unsigned s = smem_u32(reinterpret_cast<unsigned char *>(dst) + 16 * pc);
@@ -211,10 +200,10 @@ __device__ __noinline__ void merge_marked(int K, int rows, float *G, int gs, con
     }
 }
 
-// Zero `n` staged rows of `row_bytes` (a multiple of 16) starting at row pointer p.
-__device__ __forceinline__ void zero_rows(void *p, int n, int row_bytes, int lane) {
+// Zero `n` staged rows (80 B each) starting at row pointer p.
+__device__ __forceinline__ void zero_rows(void *p, int n, int lane) {
     uint4 *q = reinterpret_cast<uint4 *>(p);
-    for (int i = lane; i < n * (row_bytes >> 4); i += 32) q[i] = make_uint4(0u, 0u, 0u, 0u);
+    for (int i = lane; i < n * 5; i += 32) q[i] = make_uint4(0u, 0u, 0u, 0u);
 }
 
 // ---- BF16 tables ----
@@ -237,9 +226,8 @@ __device__ __noinline__ bool repel_bf16(const TrainArgs &a, const Geom &geo, uns
     T *w_in = static_cast<T *>(a.w_in);
     T *w_out = static_cast<T *>(a.w_out);
     const int ld = a.ld;
-    const int S = geo.stride, CW = geo.cols;             // staged row stride, columns per chunk
-    T *sin = reinterpret_cast<T *>(region + geo.stage);  // kRows x S
-    T *sout = sin + (size_t) kRows * S;                  // 16*mt x S
+    T *sin = reinterpret_cast<T *>(region + geo.stage);  // kRows x kStride
+    T *sout = sin + (size_t) kRows * kStride;            // 16*mt x kStride
     T *Gb = reinterpret_cast<T *>(region + geo.gb);      // 16*mt x kGbStride
     float *Gf = reinterpret_cast<float *>(region + geo.gf);  // K x kRows
     const int g = lane >> 2, t = lane & 3;
@@ -262,9 +250,9 @@ __device__ __noinline__ bool repel_bf16(const TrainArgs &a, const Geom &geo, uns
 #pragma unroll
                 for (int e = 0; e < 4; e++) acc[i][j][e] = 0.f;
 #pragma unroll 1
-        for (int col0 = 0; col0 < ld; col0 += CW) {
-            const int ncols = min(CW, ld - col0);
-            if (!(ok = stage_rows(st, w_in_c, w_out_c, ld, col0, ncols, sbw, rows, negs + k0, nk, sin, sout, S,
+        for (int col0 = 0; col0 < ld; col0 += kCols) {
+            const int ncols = min(kCols, ld - col0);
+            if (!(ok = stage_rows(st, w_in_c, w_out_c, ld, col0, ncols, sbw, rows, negs + k0, nk, sin, sout, kStride,
                                   lane)))
                 break;
             // rows beyond `rows` / `nk` in the tiles hold stale data; they only reach accumulator
@@ -276,7 +264,7 @@ __device__ __noinline__ bool repel_bf16(const TrainArgs &a, const Geom &geo, uns
                 for (int np = 0; np < 2; np++) {  // n-tiles 2np, 2np+1 in one ldmatrix.x4
                     unsigned r[4];
                     const int n = np * 16 + (lane & 7) + ((lane >> 4) << 3);
-                    ldsm_x4(r, sin + (size_t) n * S + ks * 16 + ((lane >> 3) & 1) * 8);
+                    ldsm_x4(r, sin + (size_t) n * kStride + ks * 16 + ((lane >> 3) & 1) * 8);
                     bfr[2 * np][0] = r[0];
                     bfr[2 * np][1] = r[1];
                     bfr[2 * np + 1][0] = r[2];
@@ -286,7 +274,7 @@ __device__ __noinline__ bool repel_bf16(const TrainArgs &a, const Geom &geo, uns
                 for (int mt = 0; mt < 3; mt++)
                     if (mt < mts) {
                         unsigned af[4];
-                        ldsm_x4(af, sout + (size_t) (mt * 16 + (lane & 15)) * S + ks * 16 + (lane >> 4) * 8);
+                        ldsm_x4(af, sout + (size_t) (mt * 16 + (lane & 15)) * kStride + ks * 16 + (lane >> 4) * 8);
 #pragma unroll
                         for (int nt = 0; nt < 4; nt++)
                             if (nt < nt1) mma16816(acc[mt][nt], af, bfr[nt][0], bfr[nt][1]);
@@ -323,8 +311,8 @@ __device__ __noinline__ bool repel_bf16(const TrainArgs &a, const Geom &geo, uns
     __syncwarp();  // the FP32 G may share the staging bytes zeroed next
     // zero the padding rows the pass-2 products read as their k dimension (they stay zero: the
     // stores write zeros back into them)
-    zero_rows(sin + (size_t) rows * S, rp - rows, S * 2, lane);
-    zero_rows(sout + (size_t) K * S, kp - K, S * 2, lane);
+    zero_rows(sin + (size_t) rows * kStride, rp - rows, lane);
+    zero_rows(sout + (size_t) K * kStride, kp - K, lane);
     __syncwarp();
 
     // ---- pass 2 ----
@@ -339,9 +327,9 @@ __device__ __noinline__ bool repel_bf16(const TrainArgs &a, const Geom &geo, uns
     const int a_row = (lane & 7) + ((lane >> 4) << 3), a_col = ((lane >> 3) & 1) * 8;
     const int s_row = lane & 7, s_col = ((lane >> 3) & 1) * 8;
 #pragma unroll 1
-    for (int col0 = 0; col0 < ld; col0 += CW) {
-        const int ncols = min(CW, ld - col0);
-        if (!stage_rows(st, w_in_c, w_out_c, ld, col0, ncols, sbw, rows, negs, K, sin, sout, S, lane))
+    for (int col0 = 0; col0 < ld; col0 += kCols) {
+        const int ncols = min(kCols, ld - col0);
+        if (!stage_rows(st, w_in_c, w_out_c, ld, col0, ncols, sbw, rows, negs, K, sin, sout, kStride, lane))
             return false;
 #pragma unroll 1
         for (int c = 0; c < ncols; c += 16) {
@@ -354,7 +342,7 @@ __device__ __noinline__ bool repel_bf16(const TrainArgs &a, const Geom &geo, uns
 #pragma unroll 1
             for (int ks = 0; ks < ksq; ks++) {
                 unsigned af[4];
-                ldsm_x4_t(af, sout + (size_t) (16 * ks + a_row) * S + c + a_col);
+                ldsm_x4_t(af, sout + (size_t) (16 * ks + a_row) * kStride + c + a_col);
 #pragma unroll
                 for (int np = 0; np < 2; np++)
                     if (2 * np < ntq) {
@@ -368,14 +356,14 @@ __device__ __noinline__ bool repel_bf16(const TrainArgs &a, const Geom &geo, uns
             for (int nt = 0; nt < 4; nt++)
                 if (nt < ntq) {
                     unsigned b[2];
-                    ldsm_x2(b, sin + (size_t) (8 * nt + s_row) * S + c + s_col);
+                    ldsm_x2(b, sin + (size_t) (8 * nt + s_row) * kStride + c + s_col);
                     mma16816(q[nt], ident, b[0], b[1]);
                 }
             // new M_out^T in groups of 6 n-tiles (48 negatives)
             unsigned ai[2][4];
 #pragma unroll
             for (int ks = 0; ks < 2; ks++)
-                if (ks < kso) ldsm_x4_t(ai[ks], sin + (size_t) (16 * ks + a_row) * S + c + a_col);
+                if (ks < kso) ldsm_x4_t(ai[ks], sin + (size_t) (16 * ks + a_row) * kStride + c + a_col);
 #pragma unroll 1
             for (int n0 = 0; n0 < nto; n0 += 6) {
                 float o[6][4];
@@ -390,7 +378,7 @@ __device__ __noinline__ bool repel_bf16(const TrainArgs &a, const Geom &geo, uns
                         mma16816(o[j], ai[0], b[0], b[1]);
                         if (kso > 1) mma16816(o[j], ai[1], b[2], b[3]);
                         unsigned bo[2];
-                        ldsm_x2(bo, sout + (size_t) (8 * nt + s_row) * S + c + s_col);
+                        ldsm_x2(bo, sout + (size_t) (8 * nt + s_row) * kStride + c + s_col);
                         mma16816(o[j], ident, bo[0], bo[1]);
                     }
                 }
@@ -401,7 +389,7 @@ __device__ __noinline__ bool repel_bf16(const TrainArgs &a, const Geom &geo, uns
                         const uint64_t bits = rb.next();
                         const unsigned p0 = pack_sr2(make_float2(o[j][0], o[j][1]), bits);
                         const unsigned p1 = pack_sr2(make_float2(o[j][2], o[j][3]), bits >> 32);
-                        stsm_x2_t(sout + (size_t) (8 * nt + s_row) * S + c + s_col, p0, p1);
+                        stsm_x2_t(sout + (size_t) (8 * nt + s_row) * kStride + c + s_col, p0, p1);
                     }
                 }
             }
@@ -411,7 +399,7 @@ __device__ __noinline__ bool repel_bf16(const TrainArgs &a, const Geom &geo, uns
                     const uint64_t bits = rb.next();
                     const unsigned p0 = pack_sr2(make_float2(q[nt][0], q[nt][1]), bits);
                     const unsigned p1 = pack_sr2(make_float2(q[nt][2], q[nt][3]), bits >> 32);
-                    stsm_x2_t(sin + (size_t) (8 * nt + s_row) * S + c + s_col, p0, p1);
+                    stsm_x2_t(sin + (size_t) (8 * nt + s_row) * kStride + c + s_col, p0, p1);
                 }
         }
         __syncwarp();
@@ -423,18 +411,18 @@ __device__ __noinline__ bool repel_bf16(const TrainArgs &a, const Geom &geo, uns
             for (int rr = lane; rr < rows + K; rr += 32) {
                 const bool is_in = rr < rows;
                 if (dup[is_in ? K + rr : rr - rows] >= 0) continue;
-                const T *src = is_in ? sin + (size_t) rr * S : sout + (size_t) (rr - rows) * S;
+                const T *src = is_in ? sin + (size_t) rr * kStride : sout + (size_t) (rr - rows) * kStride;
                 T *dst = (is_in ? w_in + (size_t) sbw[rr] * ld : w_out + (size_t) negs[rr - rows] * ld) + col0;
                 bulk_store(dst, src, (unsigned) ncols * 2u);
             }
             bulk_commit();
         } else {
-            const unsigned pieces = (unsigned) ncols / 8u, inv = 0xFFFFFFFFu / pieces + 1u;  // 16-byte pieces per row
-            for (unsigned it = lane; it < (unsigned) (rows + K) * pieces; it += 32) {
-                const int rr = (int) __umulhi(it, inv), pc = (int) (it - (unsigned) rr * pieces);
+            const int psh = ncols == 32 ? 2 : 1;  // 16-byte pieces per row: ncols / 8
+            for (int it = lane; it < (rows + K) << psh; it += 32) {
+                const int rr = it >> psh, pc = it & ((1 << psh) - 1);
                 const bool is_in = rr < rows;
                 if (dup[is_in ? K + rr : rr - rows] >= 0) continue;
-                const T *src = (is_in ? sin + (size_t) rr * S : sout + (size_t) (rr - rows) * S) + pc * 8;
+                const T *src = (is_in ? sin + (size_t) rr * kStride : sout + (size_t) (rr - rows) * kStride) + pc * 8;
                 T *dst = (is_in ? w_in + (size_t) sbw[rr] * ld : w_out + (size_t) negs[rr - rows] * ld) + col0 + pc * 8;
                 *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(src);
             }
@@ -464,9 +452,8 @@ __device__ __noinline__ bool repel_f32(const TrainArgs &a, const Geom &geo, unsi
     float *w_in = static_cast<float *>(a.w_in);
     float *w_out = static_cast<float *>(a.w_out);
     const int ld = a.ld;
-    const int S = geo.stride, CW = geo.cols;                     // staged row stride, columns per chunk
-    float *sin = reinterpret_cast<float *>(region + geo.stage);  // kRows x S
-    float *sout = sin + (size_t) kRows * S;                      // 16*mt x S
+    float *sin = reinterpret_cast<float *>(region + geo.stage);  // kRows x kF32Stride
+    float *sout = sin + (size_t) kRows * kF32Stride;             // 16*mt x kF32Stride
     float *Gp = reinterpret_cast<float *>(region + geo.gb);      // 16*mt x kGps
     float *Gf = reinterpret_cast<float *>(region + geo.gf);      // K x kRows
     const int g = lane >> 2, t = lane & 3;
@@ -489,10 +476,10 @@ __device__ __noinline__ bool repel_f32(const TrainArgs &a, const Geom &geo, unsi
 #pragma unroll
                 for (int e = 0; e < 4; e++) acc[i][j][e] = 0.f;
 #pragma unroll 1
-        for (int col0 = 0; col0 < ld; col0 += CW) {
-            const int ncols = min(CW, ld - col0);
+        for (int col0 = 0; col0 < ld; col0 += kF32Cols) {
+            const int ncols = min(kF32Cols, ld - col0);
             if (!(ok = stage_rows(st, w_in_c, w_out_c, ld, col0, ncols, sbw, rows, negs + k0, nk, sin, sout,
-                                  S, lane)))
+                                  kF32Stride, lane)))
                 break;
 #pragma unroll 1
             for (int ks = 0; ks < (ncols >> 3); ks++) {
@@ -501,7 +488,7 @@ __device__ __noinline__ bool repel_f32(const TrainArgs &a, const Geom &geo, unsi
                 for (int np = 0; np < 2; np++) {  // n-tiles 2np, 2np+1 in one ldmatrix.x4
                     float r[4];
                     const int n = np * 16 + (lane & 7) + ((lane >> 4) << 3);
-                    ldsm_x4_f32(r, sin + (size_t) n * S + ks * 8 + ((lane >> 3) & 1) * 4);
+                    ldsm_x4_f32(r, sin + (size_t) n * kF32Stride + ks * 8 + ((lane >> 3) & 1) * 4);
 #pragma unroll
                     for (int h = 0; h < 2; h++) {
                         split_tf32(r[2 * h], bb[2 * np + h][0], bs[2 * np + h][0]);
@@ -512,7 +499,7 @@ __device__ __noinline__ bool repel_f32(const TrainArgs &a, const Geom &geo, unsi
                 for (int mt = 0; mt < 3; mt++)
                     if (mt < mts) {
                         float af[4];
-                        ldsm_x4_f32(af, sout + (size_t) (mt * 16 + (lane & 7) + ((lane >> 3) & 1) * 8) * S +
+                        ldsm_x4_f32(af, sout + (size_t) (mt * 16 + (lane & 7) + ((lane >> 3) & 1) * 8) * kF32Stride +
                                             ks * 8 + (lane >> 4) * 4);
                         unsigned ab[4], as[4];
                         split_a(af, ab, as);
@@ -546,13 +533,13 @@ __device__ __noinline__ bool repel_f32(const TrainArgs &a, const Geom &geo, unsi
     }
     __syncwarp();  // the FP32 G may share the staging bytes zeroed next
     // padding rows the products read as their k dimension (8-row steps)
-    zero_rows(sin + (size_t) rows * S, 8 * kr8 - rows, S * 4, lane);
-    zero_rows(sout + (size_t) K * S, 16 * mt1 - K, S * 4, lane);
+    zero_rows(sin + (size_t) rows * kF32Stride, 8 * kr8 - rows, lane);
+    zero_rows(sout + (size_t) K * kF32Stride, 16 * mt1 - K, lane);
     __syncwarp();
 #pragma unroll 1
-    for (int col0 = 0; col0 < ld; col0 += CW) {
-        const int ncols = min(CW, ld - col0);
-        if (!stage_rows(st, w_in_c, w_out_c, ld, col0, ncols, sbw, rows, negs, K, sin, sout, S, lane))
+    for (int col0 = 0; col0 < ld; col0 += kF32Cols) {
+        const int ncols = min(kF32Cols, ld - col0);
+        if (!stage_rows(st, w_in_c, w_out_c, ld, col0, ncols, sbw, rows, negs, K, sin, sout, kF32Stride, lane))
             return false;
 #pragma unroll 1
         for (int nt = 0; nt < (ncols >> 3); nt++) {
@@ -568,8 +555,8 @@ __device__ __noinline__ bool repel_f32(const TrainArgs &a, const Geom &geo, unsi
 #pragma unroll 1
             for (int ks = 0; ks < kr8; ks++) {
                 unsigned bb[2], bs[2];
-                split_tf32(sin[(size_t) (ks * 8 + t) * S + cb + g], bb[0], bs[0]);
-                split_tf32(sin[(size_t) (ks * 8 + t + 4) * S + cb + g], bb[1], bs[1]);
+                split_tf32(sin[(size_t) (ks * 8 + t) * kF32Stride + cb + g], bb[0], bs[0]);
+                split_tf32(sin[(size_t) (ks * 8 + t + 4) * kF32Stride + cb + g], bb[1], bs[1]);
 #pragma unroll
                 for (int mt = 0; mt < MTC; mt++)
                     if (mt < mt1) {
@@ -585,8 +572,8 @@ __device__ __noinline__ bool repel_f32(const TrainArgs &a, const Geom &geo, unsi
 #pragma unroll 1
             for (int ks = 0; ks < kk8; ks++) {
                 unsigned bb[2], bs[2];
-                split_tf32(sout[(size_t) (ks * 8 + t) * S + cb + g], bb[0], bs[0]);
-                split_tf32(sout[(size_t) (ks * 8 + t + 4) * S + cb + g], bb[1], bs[1]);
+                split_tf32(sout[(size_t) (ks * 8 + t) * kF32Stride + cb + g], bb[0], bs[0]);
+                split_tf32(sout[(size_t) (ks * 8 + t + 4) * kF32Stride + cb + g], bb[1], bs[1]);
 #pragma unroll
                 for (int mt = 0; mt < 2; mt++)
                     if (mt < mr) {
@@ -606,7 +593,7 @@ __device__ __noinline__ bool repel_f32(const TrainArgs &a, const Geom &geo, unsi
                     for (int h = 0; h < 2; h++) {
                         const int row = mt * 16 + g + 8 * h;
                         if (row < K && dup[row] < 0) {
-                            const float2 old = *reinterpret_cast<const float2 *>(sout + (size_t) row * S + c);
+                            const float2 old = *reinterpret_cast<const float2 *>(sout + (size_t) row * kF32Stride + c);
                             *reinterpret_cast<float2 *>(w_out + (size_t) negs[row] * ld + col0 + c) =
                                 make_float2(old.x + o[mt][2 * h], old.y + o[mt][2 * h + 1]);
                         }
@@ -618,7 +605,7 @@ __device__ __noinline__ bool repel_f32(const TrainArgs &a, const Geom &geo, unsi
                     for (int h = 0; h < 2; h++) {
                         const int row = mt * 16 + g + 8 * h;
                         if (row < rows && dup[K + row] < 0) {
-                            const float2 old = *reinterpret_cast<const float2 *>(sin + (size_t) row * S + c);
+                            const float2 old = *reinterpret_cast<const float2 *>(sin + (size_t) row * kF32Stride + c);
                             *reinterpret_cast<float2 *>(w_in + (size_t) sbw[row] * ld + col0 + c) =
                                 make_float2(old.x + q[mt][2 * h], old.y + q[mt][2 * h + 1]);
                         }

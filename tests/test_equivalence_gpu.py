@@ -11,11 +11,10 @@ import par_word2vec_b200 as pw
 pytestmark = pytest.mark.gpu
 
 
-def run(golden, mode, attraction=pw.ATTRACT_SEQUENTIAL, variant=pw.VARIANT_AUTO, staging=pw.STAGING_AUTO, **over):
+def run(golden, mode, attraction=pw.ATTRACT_SEQUENTIAL, variant=pw.VARIANT_AUTO, **over):
     k = golden.train_kwargs()
     k.update(over)
-    with pw.Trainer(mode=mode, seed=3, grid=1, warps_per_cta=1, attraction=attraction, variant=variant,
-                    staging=staging, **k) as t:
+    with pw.Trainer(mode=mode, seed=3, grid=1, warps_per_cta=1, attraction=attraction, variant=variant, **k) as t:
         t.set_vocab(golden.counts)
         t.init_weights()
         t.set_corpus(golden.stream[:-1])
@@ -23,17 +22,15 @@ def run(golden, mode, attraction=pw.ATTRACT_SEQUENTIAL, variant=pw.VARIANT_AUTO,
         return st, t.get_weights()
 
 
-@pytest.mark.parametrize("staging", [pw.STAGING_CPASYNC, pw.STAGING_ROWS, pw.STAGING_BULK])
 @pytest.mark.parametrize("variant", [pw.VARIANT_WINDOW, pw.VARIANT_STREAM])
 @pytest.mark.parametrize("attraction", [pw.ATTRACT_SEQUENTIAL, pw.ATTRACT_WINDOW, pw.ATTRACT_PIPELINED])
 @pytest.mark.parametrize("case", ["text_small", "graph_small", "edge", "d100"])
-def test_batched_fp32_equals_plain_sequentially(golden_cases, case, attraction, variant, staging):
+def test_batched_fp32_equals_plain_sequentially(golden_cases, case, attraction, variant):
     """PIPELINED (streamed kernel) computes SEQUENTIAL's updates: PLAIN, which runs SEQUENTIAL
-    for it, is the reference for both.  The staging (64-byte chunks by cp.async or bulk copies, or
-    whole rows) does not change the result."""
+    for it, is the reference for both."""
     g = golden_cases[case]
     sp, (pi, po) = run(g, pw.MODE_PLAIN, attraction)
-    sb, (bi, bo) = run(g, pw.MODE_BATCHED, attraction, variant, staging)
+    sb, (bi, bo) = run(g, pw.MODE_BATCHED, attraction, variant)
     for k in ("kept", "sentences", "pairs", "batches", "negatives"):
         assert sp[k] == sb[k], k
     scale = max(np.abs(pi).max(), np.abs(po).max())
@@ -43,16 +40,15 @@ def test_batched_fp32_equals_plain_sequentially(golden_cases, case, attraction, 
     assert err_in < 1e-4 and err_out < 1e-4
 
 
-@pytest.mark.parametrize("staging", [pw.STAGING_CPASYNC, pw.STAGING_ROWS, pw.STAGING_BULK])
 @pytest.mark.parametrize("variant", [pw.VARIANT_WINDOW, pw.VARIANT_STREAM])
 @pytest.mark.parametrize("attraction", [pw.ATTRACT_SEQUENTIAL, pw.ATTRACT_WINDOW, pw.ATTRACT_PIPELINED])
 @pytest.mark.parametrize("case", ["text_small", "d100"])
-def test_batched_bf16_tracks_plain_sequentially(golden_cases, case, attraction, variant, staging):
+def test_batched_bf16_tracks_plain_sequentially(golden_cases, case, attraction, variant):
     """BF16 tables with stochastic rounding (and, for these shapes, the tensor-core repulsion)
     stay within a few percent of the FP32 run that makes the same random decisions."""
     g = golden_cases[case]
     _, (pi, po) = run(g, pw.MODE_PLAIN, attraction)
-    _, (bi, bo) = run(g, pw.MODE_BATCHED_BF16, attraction, variant, staging)
+    _, (bi, bo) = run(g, pw.MODE_BATCHED_BF16, attraction, variant)
     rel = np.linalg.norm(bi - pi) / np.linalg.norm(pi)
     print(case, "BF16 relative Frobenius error of W_in", rel)
     assert rel < 0.05
