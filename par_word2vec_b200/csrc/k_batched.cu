@@ -43,8 +43,6 @@ constexpr int kRing = kPrefetch + 1;          // landing buffers for targets / B
 constexpr int kMaxWarpsB = 16;
 constexpr size_t kSmemBudget = 227 * 1024;
 
-__host__ __device__ constexpr size_t up16_c(size_t x) { return (x + 15) & ~(size_t) 15; }
-
 struct Layout {  // per-warp shared-memory carve-up, in bytes (all offsets 16-byte aligned)
     int ws;            // window slots 2w+1+P
     int ch;            // repulsion column chunk (multiple of 4), CUDA-core path

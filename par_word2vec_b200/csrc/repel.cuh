@@ -11,11 +11,11 @@
 //   pass 2  re-stage each chunk (the rows' current values: "current value + own update", a
 //           one-chunk read-to-write window like the reference's unsynchronised `+=`), form the new
 //           values on the tensor cores and store them back.
-// Staging is one bulk copy (cp.async.bulk, the TMA unit) per row and chunk completing on the
-// warp's mbarrier, and the BF16 write-back one bulk store per row and chunk; or, selectable for
-// comparison, 16-byte cp.async copies and 16-byte stores.  Rows of the tables are
-// never read through this SM's L1 (bulk copies and cp.async.cg read at L2): L1 is not coherent
-// with the other SMs' writes.
+// Staging is 16-byte cp.async copies and the BF16 write-back 16-byte stores (the default); or,
+// selectable, one bulk copy (cp.async.bulk, the TMA unit) per row and chunk completing on the
+// warp's mbarrier and one bulk store per row and chunk.  Both read each row's address from a
+// per-batch table in shared memory.  Rows of the tables are never read through this SM's L1
+// (bulk copies and cp.async.cg read at L2): L1 is not coherent with the other SMs' writes.
 #pragma once
 #include <cstdint>
 
@@ -49,6 +49,7 @@ struct Geom {
     size_t stage;   // staging: kRows batch rows, then 16 * mt negative rows, 80 B each
     size_t gb;      // G kept through pass 2: BF16 16*mt x kGbStride, or FP32 16*mt x kGps
     size_t gf;      // FP32 G, kcap x kRows, for the table lookup and merging (may alias the staging)
+    size_t tab;     // row addresses: kRows batch rows, then kcap negatives (8 B each)
     size_t bytes;   // region size
 };
 
@@ -72,7 +73,8 @@ __host__ __device__ inline Geom make_geom(int window, int negative, int batch, b
         g.gf = stage_bytes;
         g.gb = stage_bytes + gf_bytes;
     }
-    g.bytes = g.gb + gb_bytes;
+    g.tab = g.gb + gb_bytes;
+    g.bytes = g.tab + up16((size_t) (kRows + g.kcap) * 8);
     return g;
 }
 
@@ -83,14 +85,38 @@ struct Stager {
     bool bulk;
 };
 
-// Stage columns [col0, col0 + ncols) of the batch rows (words sbw[0..rows)) into `sin` and of the
-// negatives negs[0..nk) into `sout` (row stride kStride BF16 = 80 B).  ncols * esz is a multiple
-// of 16 bytes.  Returns false (warp-uniform) if a bulk copy did not complete in time.
+// Global addresses of the batch's rows: tab[r] = W_in row of sbw[r] (r < rows), tab[rows + k] =
+// W_out row of negs[k] (k < K).  Bit 0 is set later on rows whose update merges into an earlier
+// copy of the same word (they are staged but not written back); rows start on 16-byte boundaries.
 template <typename T>
-__device__ __forceinline__ bool stage_rows(Stager &st, const T *w_in, const T *w_out, int ld, int col0, int ncols,
-                                           const int *sbw, int rows, const int *negs, int nk, T *sin, T *sout,
-                                           int stride, int lane) {
-    const unsigned bytes = (unsigned) ncols * (unsigned) sizeof(T);
+__device__ __forceinline__ void build_row_table(const T *w_in, const T *w_out, int ld, const int *sbw, int rows,
+                                                const int *negs, int K, uint64_t *tab, int lane) {
+    for (int i = lane; i < rows + K; i += 32) {
+        const T *p = i < rows ? w_in + (size_t) sbw[i] * ld : w_out + (size_t) negs[i - rows] * ld;
+        tab[i] = reinterpret_cast<uint64_t>(p);
+    }
+    __syncwarp();
+}
+
+// Tag the rows that mark_repeats_warp found repeated (dup[k] for negatives, dup[K + r] for batch
+// rows): the write-back skips them.
+__device__ __forceinline__ void tag_repeats(uint64_t *tab, const int *dup, int rows, int K, int lane) {
+    for (int i = lane; i < rows + K; i += 32)
+        if (dup[i < rows ? K + i : i - rows] >= 0) tab[i] |= 1u;
+    __syncwarp();
+}
+
+// Staged rows are 80 bytes apart (kStride BF16 / kF32Stride FP32).
+constexpr int kStageRowBytes = kStride * 2;
+
+// Stage bytes [c0, c0 + bytes) of the batch rows (tab[0..rows)) into `sin` and of the negatives
+// k0..k0+nk-1 (tab[rows + k0 ..]) into `sout`.  bytes is 32 or 64: each lane copies the same
+// 16-byte piece (lane mod pieces) of every (32 / pieces)-th row, so a copy costs a table read and
+// two adds.  Returns false (warp-uniform) if a bulk copy did not complete in time.
+__device__ __forceinline__ bool stage_rows(Stager &st, const uint64_t *tab, unsigned c0, unsigned bytes, int rows,
+                                           int k0, int nk, void *sin, void *sout, int lane) {
+    unsigned char *s_in = static_cast<unsigned char *>(sin), *s_out = static_cast<unsigned char *>(sout);
+    const uint64_t *t_out = tab + rows + k0;
     bool ok = true;
     if (st.bulk) {
         // the previous chunk's bulk stores have read the staging; earlier generic accesses of the
@@ -100,9 +126,10 @@ __device__ __forceinline__ bool stage_rows(Stager &st, const T *w_in, const T *w
         __syncwarp();
         if (lane == 0) mbar_arrive_expect_tx(st.bar, (unsigned) (rows + nk) * bytes);
         for (int r = lane; r < rows + nk; r += 32) {
-            const T *src = r < rows ? w_in + (size_t) sbw[r] * ld : w_out + (size_t) negs[r - rows] * ld;
-            T *dst = r < rows ? sin + (size_t) r * stride : sout + (size_t) (r - rows) * stride;
-            bulk_load(dst, src + col0, bytes, st.bar);
+            const bool in = r < rows;
+            const uint64_t src = (in ? tab[r] : t_out[r - rows]) & ~(uint64_t) 1;
+            unsigned char *dst = in ? s_in + r * kStageRowBytes : s_out + (r - rows) * kStageRowBytes;
+            bulk_load(dst, reinterpret_cast<const void *>(src + c0), bytes, st.bar);
         }
         ok = __all_sync(0xffffffffu, mbar_wait_bounded(st.bar, st.phase, kMaxBulkPolls));
         // a copy that did not complete in time: wait once more (bounded) for the copies in flight
@@ -110,17 +137,18 @@ __device__ __forceinline__ bool stage_rows(Stager &st, const T *w_in, const T *w
         if (!ok) mbar_wait_bounded(st.bar, st.phase, kMaxBulkPolls);
         st.phase ^= 1u;
     } else {
-        const int pieces = (int) (bytes / 16);
-        const int shift = pieces == 4 ? 2 : (pieces == 2 ? 1 : 0);  // pieces per row: 1, 2 or 4
-        for (int it = lane; it < (rows + nk) << shift; it += 32) {
-            const int r = it >> shift, pc = it & (pieces - 1);
-            const T *src = r < rows ? w_in + (size_t) sbw[r] * ld : w_out + (size_t) negs[r - rows] * ld;
-            T *dst = r < rows ? sin + (size_t) r * stride : sout + (size_t) (r - rows) * stride;
-            const unsigned s = smem_u32(reinterpret_cast<unsigned char *>(dst) + 16 * pc);
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s),
-                         "l"(reinterpret_cast<const unsigned char *>(src + col0) + 16 * pc)
+        const int sh = bytes == 64u ? 2 : 1;  // log2 of the 16-byte pieces per row
+        const int r0 = lane >> sh, step = 32 >> sh;
+        const unsigned pc16 = 16u * (unsigned) (lane & ((1 << sh) - 1));
+        const uint64_t goff = c0 + pc16;
+        unsigned s = smem_u32(s_in) + (unsigned) r0 * kStageRowBytes + pc16;
+        for (int r = r0; r < rows; r += step, s += step * kStageRowBytes)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"((tab[r] & ~(uint64_t) 1) + goff)
                          : "memory");
-        }
+        s = smem_u32(s_out) + (unsigned) r0 * kStageRowBytes + pc16;
+        for (int r = r0; r < nk; r += step, s += step * kStageRowBytes)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"((t_out[r] & ~(uint64_t) 1) + goff)
+                         : "memory");
         asm volatile("cp.async.commit_group;" ::: "memory");
         asm volatile("cp.async.wait_group 0;" ::: "memory");
     }
@@ -223,8 +251,6 @@ __device__ __noinline__ bool repel_bf16(const TrainArgs &a, const Geom &geo, uns
     using T = __nv_bfloat16;
     const T *w_in_c = static_cast<const T *>(a.w_in);
     const T *w_out_c = static_cast<const T *>(a.w_out);
-    T *w_in = static_cast<T *>(a.w_in);
-    T *w_out = static_cast<T *>(a.w_out);
     const int ld = a.ld;
     T *sin = reinterpret_cast<T *>(region + geo.stage);  // kRows x kStride
     T *sout = sin + (size_t) kRows * kStride;            // 16*mt x kStride
@@ -232,6 +258,8 @@ __device__ __noinline__ bool repel_bf16(const TrainArgs &a, const Geom &geo, uns
     float *Gf = reinterpret_cast<float *>(region + geo.gf);  // K x kRows
     const int g = lane >> 2, t = lane & 3;
     const int nt1 = (rows + 7) >> 3;  // pass 1: n-tiles of batch rows
+    uint64_t *tab = reinterpret_cast<uint64_t *>(region + geo.tab);
+    build_row_table(w_in_c, w_out_c, ld, sbw, rows, negs, K, tab, lane);
     bool ok = true;
     // this warp's earlier plain stores to the tables (the sentence's attraction, the previous
     // batch's write-back) before the bulk copies read the same rows
@@ -252,9 +280,7 @@ __device__ __noinline__ bool repel_bf16(const TrainArgs &a, const Geom &geo, uns
 #pragma unroll 1
         for (int col0 = 0; col0 < ld; col0 += kCols) {
             const int ncols = min(kCols, ld - col0);
-            if (!(ok = stage_rows(st, w_in_c, w_out_c, ld, col0, ncols, sbw, rows, negs + k0, nk, sin, sout, kStride,
-                                  lane)))
-                break;
+            if (!(ok = stage_rows(st, tab, 2u * col0, 2u * ncols, rows, k0, nk, sin, sout, lane))) break;
             // rows beyond `rows` / `nk` in the tiles hold stale data; they only reach accumulator
             // entries that are never read
 #pragma unroll 1
@@ -299,6 +325,7 @@ __device__ __noinline__ bool repel_bf16(const TrainArgs &a, const Geom &geo, uns
     if (!ok) return false;
     mark_repeats_warp(negs, K, sbw, rows, dup, lane);
     merge_marked(K, rows, Gf, kRows, dup, lane);
+    tag_repeats(tab, dup, rows, K, lane);
     // BF16 G, zero outside K x rows up to whole 16 x 16 blocks
     const int kp = 16 * ((K + 15) >> 4), rp = 16 * ((rows + 15) >> 4);
     const int hsh = rp == 32 ? 4 : 3;  // column pairs per G row: rp / 2
@@ -329,78 +356,69 @@ __device__ __noinline__ bool repel_bf16(const TrainArgs &a, const Geom &geo, uns
 #pragma unroll 1
     for (int col0 = 0; col0 < ld; col0 += kCols) {
         const int ncols = min(kCols, ld - col0);
-        if (!stage_rows(st, w_in_c, w_out_c, ld, col0, ncols, sbw, rows, negs, K, sin, sout, kStride, lane))
-            return false;
+        if (!stage_rows(st, tab, 2u * col0, 2u * ncols, rows, 0, K, sin, sout, lane)) return false;
 #pragma unroll 1
         for (int c = 0; c < ncols; c += 16) {
-            // new M_in^T slices: q[nt] covers batch rows 8nt..8nt+7 of these 16 columns
-            float q[4][4];
-#pragma unroll
-            for (int nt = 0; nt < 4; nt++)
-#pragma unroll
-                for (int e = 0; e < 4; e++) q[nt][e] = 0.f;
-#pragma unroll 1
-            for (int ks = 0; ks < ksq; ks++) {
-                unsigned af[4];
-                ldsm_x4_t(af, sout + (size_t) (16 * ks + a_row) * kStride + c + a_col);
-#pragma unroll
-                for (int np = 0; np < 2; np++)
-                    if (2 * np < ntq) {
-                        unsigned b[4];  // G rows 16ks..16ks+15 at columns 16np..16np+15: n-tiles 2np, 2np+1
-                        ldsm_x4_t(b, Gb + (size_t) (16 * ks + (lane & 15)) * kGbStride + 16 * np + ((lane >> 4) << 3));
-                        mma16816(q[2 * np], af, b[0], b[1]);
-                        if (2 * np + 1 < ntq) mma16816(q[2 * np + 1], af, b[2], b[3]);
-                    }
-            }
-#pragma unroll
-            for (int nt = 0; nt < 4; nt++)
-                if (nt < ntq) {
-                    unsigned b[2];
-                    ldsm_x2(b, sin + (size_t) (8 * nt + s_row) * kStride + c + s_col);
-                    mma16816(q[nt], ident, b[0], b[1]);
-                }
-            // new M_out^T in groups of 6 n-tiles (48 negatives)
+            // the old M_in^T slices the M_out products take as A, read before the new M_in values
+            // overwrite them
             unsigned ai[2][4];
 #pragma unroll
             for (int ks = 0; ks < 2; ks++)
                 if (ks < kso) ldsm_x4_t(ai[ks], sin + (size_t) (16 * ks + a_row) * kStride + c + a_col);
+            // new M_in^T slices, two n-tiles (batch rows 16np..16np+15) at a time
 #pragma unroll 1
-            for (int n0 = 0; n0 < nto; n0 += 6) {
-                float o[6][4];
-#pragma unroll
-                for (int j = 0; j < 6; j++) {
-#pragma unroll
-                    for (int e = 0; e < 4; e++) o[j][e] = 0.f;
-                    const int nt = n0 + j;
-                    if (nt < nto) {
-                        unsigned b[4];  // G rows 8nt..8nt+7, columns 0..31 (k-steps 0 and 1)
-                        ldsm_x4(b, Gb + (size_t) (8 * nt + (lane & 7)) * kGbStride + ((lane >> 3) & 3) * 8);
-                        mma16816(o[j], ai[0], b[0], b[1]);
-                        if (kso > 1) mma16816(o[j], ai[1], b[2], b[3]);
-                        unsigned bo[2];
-                        ldsm_x2(bo, sout + (size_t) (8 * nt + s_row) * kStride + c + s_col);
-                        mma16816(o[j], ident, bo[0], bo[1]);
-                    }
+            for (int np = 0; 2 * np < ntq; np++) {
+                const bool two = 2 * np + 1 < ntq;
+                float q0[4], q1[4];
+                const T *gq = Gb + (size_t) (lane & 15) * kGbStride + 16 * np + ((lane >> 4) << 3);
+                const T *aq = sout + (size_t) a_row * kStride + c + a_col;
+                {
+                    unsigned af[4], b[4];  // k-step 0: G rows 0..15 at columns 16np..16np+15
+                    ldsm_x4_t(af, aq);
+                    ldsm_x4_t(b, gq);
+                    mma16816_z(q0, af, b[0], b[1]);
+                    if (two) mma16816_z(q1, af, b[2], b[3]);
                 }
-#pragma unroll
-                for (int j = 0; j < 6; j++) {
-                    const int nt = n0 + j;
-                    if (nt < nto) {
-                        const uint64_t bits = rb.next();
-                        const unsigned p0 = pack_sr2(make_float2(o[j][0], o[j][1]), bits);
-                        const unsigned p1 = pack_sr2(make_float2(o[j][2], o[j][3]), bits >> 32);
-                        stsm_x2_t(sout + (size_t) (8 * nt + s_row) * kStride + c + s_col, p0, p1);
-                    }
+#pragma unroll 1
+                for (int ks = 1; ks < ksq; ks++) {
+                    unsigned af[4], b[4];
+                    ldsm_x4_t(af, aq + (size_t) 16 * ks * kStride);
+                    ldsm_x4_t(b, gq + (size_t) 16 * ks * kGbStride);
+                    mma16816(q0, af, b[0], b[1]);
+                    if (two) mma16816(q1, af, b[2], b[3]);
+                }
+                T *srow = sin + (size_t) (16 * np + s_row) * kStride + c + s_col;
+                unsigned bi[2];
+                ldsm_x2(bi, srow);
+                mma16816(q0, ident, bi[0], bi[1]);
+                uint64_t bits = rb.next();
+                stsm_x2_t(srow, pack_sr2(make_float2(q0[0], q0[1]), bits), pack_sr2(make_float2(q0[2], q0[3]), bits >> 32));
+                if (two) {
+                    ldsm_x2(bi, srow + 8 * kStride);
+                    mma16816(q1, ident, bi[0], bi[1]);
+                    bits = rb.next();
+                    stsm_x2_t(srow + 8 * kStride, pack_sr2(make_float2(q1[0], q1[1]), bits),
+                              pack_sr2(make_float2(q1[2], q1[3]), bits >> 32));
                 }
             }
-#pragma unroll
-            for (int nt = 0; nt < 4; nt++)
-                if (nt < ntq) {
-                    const uint64_t bits = rb.next();
-                    const unsigned p0 = pack_sr2(make_float2(q[nt][0], q[nt][1]), bits);
-                    const unsigned p1 = pack_sr2(make_float2(q[nt][2], q[nt][3]), bits >> 32);
-                    stsm_x2_t(sin + (size_t) (8 * nt + s_row) * kStride + c + s_col, p0, p1);
-                }
+            // new M_out^T, one n-tile (8 negatives) at a time: each tile's product, sum and rounding
+            // is independent of the others
+#pragma unroll 1
+            for (int nt = 0; nt < nto; nt++) {
+                float o[4];
+                unsigned b[4];  // G rows 8nt..8nt+7, columns 0..31 (k-steps 0 and 1)
+                ldsm_x4(b, Gb + (size_t) (8 * nt + (lane & 7)) * kGbStride + ((lane >> 3) & 3) * 8);
+                mma16816_z(o, ai[0], b[0], b[1]);
+                if (kso > 1) mma16816(o, ai[1], b[2], b[3]);
+                unsigned bo[2];
+                T *srow = sout + (size_t) (8 * nt + s_row) * kStride + c + s_col;
+                ldsm_x2(bo, srow);
+                mma16816(o, ident, bo[0], bo[1]);
+                const uint64_t bits = rb.next();
+                const unsigned p0 = pack_sr2(make_float2(o[0], o[1]), bits);
+                const unsigned p1 = pack_sr2(make_float2(o[2], o[3]), bits >> 32);
+                stsm_x2_t(srow, p0, p1);
+            }
         }
         __syncwarp();
         // every distinct row's new chunk back to its table
@@ -409,22 +427,27 @@ __device__ __noinline__ bool repel_bf16(const TrainArgs &a, const Geom &geo, uns
             fence_proxy_async_shared();  // this lane's stmatrix writes before the bulk reads
             __syncwarp();
             for (int rr = lane; rr < rows + K; rr += 32) {
-                const bool is_in = rr < rows;
-                if (dup[is_in ? K + rr : rr - rows] >= 0) continue;
-                const T *src = is_in ? sin + (size_t) rr * kStride : sout + (size_t) (rr - rows) * kStride;
-                T *dst = (is_in ? w_in + (size_t) sbw[rr] * ld : w_out + (size_t) negs[rr - rows] * ld) + col0;
-                bulk_store(dst, src, (unsigned) ncols * 2u);
+                const uint64_t ad = tab[rr];
+                if (ad & 1u) continue;  // a repeated word: its first copy carries the merged update
+                const T *src = rr < rows ? sin + (size_t) rr * kStride : sout + (size_t) (rr - rows) * kStride;
+                bulk_store(reinterpret_cast<void *>(ad + 2u * col0), src, (unsigned) ncols * 2u);
             }
             bulk_commit();
         } else {
-            const int psh = ncols == 32 ? 2 : 1;  // 16-byte pieces per row: ncols / 8
-            for (int it = lane; it < (rows + K) << psh; it += 32) {
-                const int rr = it >> psh, pc = it & ((1 << psh) - 1);
-                const bool is_in = rr < rows;
-                if (dup[is_in ? K + rr : rr - rows] >= 0) continue;
-                const T *src = (is_in ? sin + (size_t) rr * kStride : sout + (size_t) (rr - rows) * kStride) + pc * 8;
-                T *dst = (is_in ? w_in + (size_t) sbw[rr] * ld : w_out + (size_t) negs[rr - rows] * ld) + col0 + pc * 8;
-                *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(src);
+            // as in stage_rows: each lane stores the same 16-byte piece of every (32 / pieces)-th row
+            const int sh = ncols == kCols ? 2 : 1;  // log2 of the 16-byte pieces per row
+            const int r0 = lane >> sh, step = 32 >> sh;
+            const unsigned pc16 = 16u * (unsigned) (lane & ((1 << sh) - 1));
+            const uint64_t goff = 2u * (unsigned) col0 + pc16;
+            const unsigned char *src = reinterpret_cast<const unsigned char *>(sin) + r0 * kStageRowBytes + pc16;
+            for (int r = r0; r < rows; r += step, src += step * kStageRowBytes) {
+                const uint64_t ad = tab[r];
+                if (!(ad & 1u)) *reinterpret_cast<uint4 *>(ad + goff) = *reinterpret_cast<const uint4 *>(src);
+            }
+            src = reinterpret_cast<const unsigned char *>(sout) + r0 * kStageRowBytes + pc16;
+            for (int r = r0; r < K; r += step, src += step * kStageRowBytes) {
+                const uint64_t ad = tab[rows + r];
+                if (!(ad & 1u)) *reinterpret_cast<uint4 *>(ad + goff) = *reinterpret_cast<const uint4 *>(src);
             }
         }
         __syncwarp();
@@ -462,6 +485,8 @@ __device__ __noinline__ bool repel_f32(const TrainArgs &a, const Geom &geo, unsi
     const int kr8 = (rows + 7) >> 3;  // 8-row k-steps over the batch rows
     const int kk8 = (K + 7) >> 3;     // 8-row k-steps over the negatives
     const int mr = (rows + 15) >> 4;  // m-tiles of batch rows (pass 2)
+    uint64_t *tab = reinterpret_cast<uint64_t *>(region + geo.tab);
+    build_row_table(w_in_c, w_out_c, ld, sbw, rows, negs, K, tab, lane);  // no tags: pass 2 writes from registers
     bool ok = true;
     if (st.bulk) fence_proxy_async_global();  // as in repel_bf16
 #pragma unroll 1
@@ -478,9 +503,7 @@ __device__ __noinline__ bool repel_f32(const TrainArgs &a, const Geom &geo, unsi
 #pragma unroll 1
         for (int col0 = 0; col0 < ld; col0 += kF32Cols) {
             const int ncols = min(kF32Cols, ld - col0);
-            if (!(ok = stage_rows(st, w_in_c, w_out_c, ld, col0, ncols, sbw, rows, negs + k0, nk, sin, sout,
-                                  kF32Stride, lane)))
-                break;
+            if (!(ok = stage_rows(st, tab, 4u * col0, 4u * ncols, rows, k0, nk, sin, sout, lane))) break;
 #pragma unroll 1
             for (int ks = 0; ks < (ncols >> 3); ks++) {
                 unsigned bb[4][2], bs[4][2];
@@ -539,8 +562,7 @@ __device__ __noinline__ bool repel_f32(const TrainArgs &a, const Geom &geo, unsi
 #pragma unroll 1
     for (int col0 = 0; col0 < ld; col0 += kF32Cols) {
         const int ncols = min(kF32Cols, ld - col0);
-        if (!stage_rows(st, w_in_c, w_out_c, ld, col0, ncols, sbw, rows, negs, K, sin, sout, kF32Stride, lane))
-            return false;
+        if (!stage_rows(st, tab, 4u * col0, 4u * ncols, rows, 0, K, sin, sout, lane)) return false;
 #pragma unroll 1
         for (int nt = 0; nt < (ncols >> 3); nt++) {
             const int cb = nt * 8;
