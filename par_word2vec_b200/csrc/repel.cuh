@@ -241,9 +241,10 @@ __device__ __forceinline__ void zero_rows(void *p, int n, int lane) {
 //   new M_out^T (16 x K)    = M_in^T (16 x rows) . G^T (rows x K) + I . M_out^T
 // The identity products add the staged values exactly in FP32, so the accumulators hold the new
 // values; each 8-row slice is rounded stochastically to BF16 and written back into the staged tile
-// with stmatrix.trans, and whole 16-byte pieces go back to the tables.  The M_in update is formed
-// first (it reads the old M_out), then the M_out update in groups of 48 negatives (each group
-// reads only old M_in and its own old rows), then the M_in result is stored.
+// with stmatrix.trans, and whole 16-byte pieces go back to the tables.  Per 16-column tile the old
+// M_in^T fragments the M_out products need are read into registers first; then the M_in update is
+// formed and stored two n-tiles at a time (it reads the old M_out), then the M_out update one
+// n-tile at a time (each tile reads only those registers and its own old rows).
 // Returns false if staging failed (the batch is then left partly applied: the caller stops).
 __device__ __noinline__ bool repel_bf16(const TrainArgs &a, const Geom &geo, unsigned char *region, const int *sbw,
                                         int rows, const int *negs, int K, float alpha, const float *s_exp, int *dup,
