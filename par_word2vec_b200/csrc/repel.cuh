@@ -13,8 +13,9 @@
 //           values on the tensor cores and store them back.
 // Staging is 16-byte cp.async copies and the BF16 write-back 16-byte stores (the default); or,
 // selectable, one bulk copy (cp.async.bulk, the TMA unit) per row and chunk completing on the
-// warp's mbarrier and one bulk store per row and chunk.  Both read each row's address from a
-// per-batch table in shared memory.  Rows of the tables are never read through this SM's L1
+// warp's mbarrier and one bulk store per row and chunk.  The BF16 path reads each row's address
+// from a per-batch table in shared memory (which also marks the rows its write-back skips); the
+// FP32 path forms them from the words.  Rows of the tables are never read through this SM's L1
 // (bulk copies and cp.async.cg read at L2): L1 is not coherent with the other SMs' writes.
 #pragma once
 #include <cstdint>
@@ -49,7 +50,7 @@ struct Geom {
     size_t stage;   // staging: kRows batch rows, then 16 * mt negative rows, 80 B each
     size_t gb;      // G kept through pass 2: BF16 16*mt x kGbStride, or FP32 16*mt x kGps
     size_t gf;      // FP32 G, kcap x kRows, for the table lookup and merging (may alias the staging)
-    size_t tab;     // row addresses: kRows batch rows, then kcap negatives (8 B each)
+    size_t tab;     // BF16: row addresses, kRows batch rows then kcap negatives (8 B each)
     size_t bytes;   // region size
 };
 
@@ -74,7 +75,9 @@ __host__ __device__ inline Geom make_geom(int window, int negative, int batch, b
         g.gb = stage_bytes + gf_bytes;
     }
     g.tab = g.gb + gb_bytes;
-    g.bytes = g.tab + up16((size_t) (kRows + g.kcap) * 8);
+    // the FP32 path forms row addresses from the words instead: without the table its warps fit
+    // 16 to an SM
+    g.bytes = g.tab + (bf16 ? up16((size_t) (kRows + g.kcap) * 8) : 0);
     return g;
 }
 
@@ -109,14 +112,31 @@ __device__ __forceinline__ void tag_repeats(uint64_t *tab, const int *dup, int r
 // Staged rows are 80 bytes apart (kStride BF16 / kF32Stride FP32).
 constexpr int kStageRowBytes = kStride * 2;
 
-// Stage bytes [c0, c0 + bytes) of the batch rows (tab[0..rows)) into `sin` and of the negatives
-// k0..k0+nk-1 (tab[rows + k0 ..]) into `sout`.  bytes is 32 or 64: each lane copies the same
-// 16-byte piece (lane mod pieces) of every (32 / pieces)-th row, so a copy costs a table read and
-// two adds.  Returns false (warp-uniform) if a bulk copy did not complete in time.
-__device__ __forceinline__ bool stage_rows(Stager &st, const uint64_t *tab, unsigned c0, unsigned bytes, int rows,
+// Where stage_rows finds a batch row r (in) and negative k (out): the BF16 path's table (tag bit
+// masked off), or the FP32 path's words and tables.
+struct RowsFromTable {
+    const uint64_t *tab;
+    int rows;
+    __device__ uint64_t in(int r) const { return tab[r] & ~(uint64_t) 1; }
+    __device__ uint64_t out(int k) const { return tab[rows + k] & ~(uint64_t) 1; }
+};
+template <typename T>
+struct RowsFromWords {
+    const T *w_in, *w_out;
+    int ld;
+    const int *sbw, *negs;
+    __device__ uint64_t in(int r) const { return reinterpret_cast<uint64_t>(w_in + (size_t) sbw[r] * ld); }
+    __device__ uint64_t out(int k) const { return reinterpret_cast<uint64_t>(w_out + (size_t) negs[k] * ld); }
+};
+
+// Stage bytes [c0, c0 + bytes) of the batch rows (rows.in(0..rows)) into `sin` and of the
+// negatives k0..k0+nk-1 (rows.out(k0..)) into `sout`.  bytes is 32 or 64: each lane copies the
+// same 16-byte piece (lane mod pieces) of every (32 / pieces)-th row.  Returns false (warp-uniform)
+// if a bulk copy did not complete in time.
+template <typename Rows>
+__device__ __forceinline__ bool stage_rows(Stager &st, const Rows &rowsrc, unsigned c0, unsigned bytes, int rows,
                                            int k0, int nk, void *sin, void *sout, int lane) {
     unsigned char *s_in = static_cast<unsigned char *>(sin), *s_out = static_cast<unsigned char *>(sout);
-    const uint64_t *t_out = tab + rows + k0;
     bool ok = true;
     if (st.bulk) {
         // the previous chunk's bulk stores have read the staging; earlier generic accesses of the
@@ -127,7 +147,7 @@ __device__ __forceinline__ bool stage_rows(Stager &st, const uint64_t *tab, unsi
         if (lane == 0) mbar_arrive_expect_tx(st.bar, (unsigned) (rows + nk) * bytes);
         for (int r = lane; r < rows + nk; r += 32) {
             const bool in = r < rows;
-            const uint64_t src = (in ? tab[r] : t_out[r - rows]) & ~(uint64_t) 1;
+            const uint64_t src = in ? rowsrc.in(r) : rowsrc.out(k0 + r - rows);
             unsigned char *dst = in ? s_in + r * kStageRowBytes : s_out + (r - rows) * kStageRowBytes;
             bulk_load(dst, reinterpret_cast<const void *>(src + c0), bytes, st.bar);
         }
@@ -143,11 +163,10 @@ __device__ __forceinline__ bool stage_rows(Stager &st, const uint64_t *tab, unsi
         const uint64_t goff = c0 + pc16;
         unsigned s = smem_u32(s_in) + (unsigned) r0 * kStageRowBytes + pc16;
         for (int r = r0; r < rows; r += step, s += step * kStageRowBytes)
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"((tab[r] & ~(uint64_t) 1) + goff)
-                         : "memory");
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(rowsrc.in(r) + goff) : "memory");
         s = smem_u32(s_out) + (unsigned) r0 * kStageRowBytes + pc16;
         for (int r = r0; r < nk; r += step, s += step * kStageRowBytes)
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"((t_out[r] & ~(uint64_t) 1) + goff)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(rowsrc.out(k0 + r) + goff)
                          : "memory");
         asm volatile("cp.async.commit_group;" ::: "memory");
         asm volatile("cp.async.wait_group 0;" ::: "memory");
@@ -281,7 +300,8 @@ __device__ __noinline__ bool repel_bf16(const TrainArgs &a, const Geom &geo, uns
 #pragma unroll 1
         for (int col0 = 0; col0 < ld; col0 += kCols) {
             const int ncols = min(kCols, ld - col0);
-            if (!(ok = stage_rows(st, tab, 2u * col0, 2u * ncols, rows, k0, nk, sin, sout, lane))) break;
+            if (!(ok = stage_rows(st, RowsFromTable{tab, rows}, 2u * col0, 2u * ncols, rows, k0, nk, sin, sout, lane)))
+                break;
             // rows beyond `rows` / `nk` in the tiles hold stale data; they only reach accumulator
             // entries that are never read
 #pragma unroll 1
@@ -357,7 +377,7 @@ __device__ __noinline__ bool repel_bf16(const TrainArgs &a, const Geom &geo, uns
 #pragma unroll 1
     for (int col0 = 0; col0 < ld; col0 += kCols) {
         const int ncols = min(kCols, ld - col0);
-        if (!stage_rows(st, tab, 2u * col0, 2u * ncols, rows, 0, K, sin, sout, lane)) return false;
+        if (!stage_rows(st, RowsFromTable{tab, rows}, 2u * col0, 2u * ncols, rows, 0, K, sin, sout, lane)) return false;
 #pragma unroll 1
         for (int c = 0; c < ncols; c += 16) {
             // the old M_in^T slices the M_out products take as A, read before the new M_in values
@@ -486,8 +506,7 @@ __device__ __noinline__ bool repel_f32(const TrainArgs &a, const Geom &geo, unsi
     const int kr8 = (rows + 7) >> 3;  // 8-row k-steps over the batch rows
     const int kk8 = (K + 7) >> 3;     // 8-row k-steps over the negatives
     const int mr = (rows + 15) >> 4;  // m-tiles of batch rows (pass 2)
-    uint64_t *tab = reinterpret_cast<uint64_t *>(region + geo.tab);
-    build_row_table(w_in_c, w_out_c, ld, sbw, rows, negs, K, tab, lane);  // no tags: pass 2 writes from registers
+    const RowsFromWords<float> rowsrc{w_in_c, w_out_c, ld, sbw, negs};
     bool ok = true;
     if (st.bulk) fence_proxy_async_global();  // as in repel_bf16
 #pragma unroll 1
@@ -504,7 +523,7 @@ __device__ __noinline__ bool repel_f32(const TrainArgs &a, const Geom &geo, unsi
 #pragma unroll 1
         for (int col0 = 0; col0 < ld; col0 += kF32Cols) {
             const int ncols = min(kF32Cols, ld - col0);
-            if (!(ok = stage_rows(st, tab, 4u * col0, 4u * ncols, rows, k0, nk, sin, sout, lane))) break;
+            if (!(ok = stage_rows(st, rowsrc, 4u * col0, 4u * ncols, rows, k0, nk, sin, sout, lane))) break;
 #pragma unroll 1
             for (int ks = 0; ks < (ncols >> 3); ks++) {
                 unsigned bb[4][2], bs[4][2];
@@ -563,7 +582,7 @@ __device__ __noinline__ bool repel_f32(const TrainArgs &a, const Geom &geo, unsi
 #pragma unroll 1
     for (int col0 = 0; col0 < ld; col0 += kF32Cols) {
         const int ncols = min(kF32Cols, ld - col0);
-        if (!stage_rows(st, tab, 4u * col0, 4u * ncols, rows, 0, K, sin, sout, lane)) return false;
+        if (!stage_rows(st, rowsrc, 4u * col0, 4u * ncols, rows, 0, K, sin, sout, lane)) return false;
 #pragma unroll 1
         for (int nt = 0; nt < (ncols >> 3); nt++) {
             const int cb = nt * 8;
