@@ -23,23 +23,46 @@ cudaError_t launch_build_thresholds(const uint32_t *counts, int V, float sample,
 // The reference fills the table sequentially: slot a gets the current word i, then i advances
 // when a / 1e8f > d1, where d1 is a float running sum of the double quotients cn^0.75 / total.
 // Word i therefore owns slots [t_i, e_i] with e_i = max(t_i, g_i), g_i the first slot whose
-// float position exceeds threshold D_i, and t_{i+1} = e_i + 1.  The two V-long recurrences
-// (the FP64 total with the float running sum, and the max-plus start recurrence) run on one
-// thread each, exactly as ordered in the reference; the 27-step threshold search per word and
-// the 1e8-slot fill run in parallel.
+// float position exceeds threshold D_i, and t_{i+1} = e_i + 1.  The FP64 total and the float
+// running sum are sequential recurrences and run in the reference's order, one addition after the
+// other, on one warp whose lanes load 32 values at a time and pass them along by shuffles (so the
+// chain never waits for memory); the quotients, the 27-step threshold search per word, the
+// max-plus start recurrence (as a prefix maximum) and the 1e8-slot fill run in parallel.
 
-// One thread: total = sum of pow_cn in index order (the reference's reduction at one thread),
-// then D_i (float), the value of d1 while word i is current.
-__global__ void k_table_thresholds(const double *pow_cn, int V, float *D, double *total_out) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// total = sum of pow_cn in index order, the reference's double additions one by one; every lane
+// runs the same chain on the shuffled values.
+__global__ void k_table_total(const double *pow_cn, int V, double *total_out) {
+    const int lane = threadIdx.x;
     double total = 0.0;
-    for (int i = 0; i < V; i++) total += pow_cn[i];
-    *total_out = total;
-    float d1 = (float) (pow_cn[0] / total);
-    D[0] = d1;
-    for (int i = 1; i < V; i++) {
-        d1 = (float) ((double) d1 + pow_cn[i] / total);
-        D[i] = d1;
+    for (int base = 0; base < V; base += 32) {
+        const double v = base + lane < V ? pow_cn[base + lane] : 0.0;
+        const int n = min(32, V - base);
+        for (int j = 0; j < n; j++) total += __shfl_sync(0xffffffffu, v, j);
+    }
+    if (lane == 0) *total_out = total;
+}
+
+// q_i = pow_cn_i / total (the same double division the recurrence below adds)
+__global__ void k_table_quotients(const double *pow_cn, int V, const double *total, double *q) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < V) q[i] = pow_cn[i] / *total;
+}
+
+// D_i, the value of the float d1 while word i is current: d1 = (float) q_0, then
+// d1 = (float) ((double) d1 + q_i), in index order; lane j keeps step j's value of each 32.
+__global__ void k_table_running(const double *q, int V, float *D) {
+    const int lane = threadIdx.x;
+    float d1 = 0.f;
+    for (int base = 0; base < V; base += 32) {
+        const double v = base + lane < V ? q[base + lane] : 0.0;
+        const int n = min(32, V - base);
+        float mine = 0.f;
+        for (int j = 0; j < n; j++) {
+            const double x = __shfl_sync(0xffffffffu, v, j);
+            d1 = base + j == 0 ? (float) x : (float) ((double) d1 + x);
+            if (lane == j) mine = d1;
+        }
+        if (lane < n) D[base + lane] = mine;
     }
 }
 
@@ -61,14 +84,32 @@ __global__ void k_table_first_slot(const float *D, int V, long long *g) {
     g[i] = lo;
 }
 
-// One thread: t_0 = 0, t_{i+1} = max(t_i, g_i) + 1, written in place over g.
-__global__ void k_table_starts(long long *g_then_t, int V) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    long long t = 0;
-    for (int i = 0; i < V; i++) {
-        long long gi = g_then_t[i];
-        g_then_t[i] = t;
-        t = (t > gi ? t : gi) + 1;
+// t_0 = 0, t_{i+1} = max(t_i, g_i) + 1, written in place over g.  With u_i = t_i - i this is
+// u_0 = 0, u_{i+1} = max(u_i, g_i - i): u_i is the exclusive prefix maximum of g_j - j (floored at
+// 0), the same integers as the one-step-at-a-time recurrence.  One block: each thread scans a
+// contiguous chunk, the chunk maxima are scanned in shared memory, then each chunk is written.
+constexpr int kStartsThreads = 1024;
+__global__ void __launch_bounds__(kStartsThreads) k_table_starts(long long *g_then_t, int V) {
+    __shared__ long long part[kStartsThreads];
+    const long long kNone = -(1LL << 62);
+    const int tid = threadIdx.x;
+    const int per = (V + kStartsThreads - 1) / kStartsThreads;
+    const int lo = min(V, tid * per), hi = min(V, lo + per);
+    long long m = kNone;  // max of g_j - j over this thread's chunk
+    for (int i = lo; i < hi; i++) m = max(m, g_then_t[i] - i);
+    part[tid] = m;
+    __syncthreads();
+    for (int off = 1; off < kStartsThreads; off <<= 1) {  // inclusive prefix maximum of the chunks
+        const long long v = tid >= off ? part[tid - off] : kNone;
+        __syncthreads();
+        part[tid] = max(part[tid], v);
+        __syncthreads();
+    }
+    long long u = tid == 0 ? 0 : max(0LL, part[tid - 1]);
+    for (int i = lo; i < hi; i++) {
+        const long long gi = g_then_t[i];
+        g_then_t[i] = i + u;
+        u = max(u, gi - i);
     }
 }
 
@@ -97,9 +138,12 @@ __global__ void k_table_fill(const long long *t, int V, int32_t *table) {
 
 cudaError_t launch_build_table(const double *pow_cn, int V, int32_t *table, float *D, long long *g,
                                double *total, cudaStream_t s) {
-    k_table_thresholds<<<1, 32, 0, s>>>(pow_cn, V, D, total);
+    double *q = reinterpret_cast<double *>(g);  // the quotients, until the first slots replace them
+    k_table_total<<<1, 32, 0, s>>>(pow_cn, V, total);
+    k_table_quotients<<<(V + 255) / 256, 256, 0, s>>>(pow_cn, V, total, q);
+    k_table_running<<<1, 32, 0, s>>>(q, V, D);
     k_table_first_slot<<<(V + 255) / 256, 256, 0, s>>>(D, V, g);
-    k_table_starts<<<1, 32, 0, s>>>(g, V);
+    k_table_starts<<<1, kStartsThreads, 0, s>>>(g, V);
     const long long chunks = (kTableSize + kFillChunk - 1) / kFillChunk;
     k_table_fill<<<(unsigned) ((chunks + 255) / 256), 256, 0, s>>>(g, V, table);
     return cudaGetLastError();
