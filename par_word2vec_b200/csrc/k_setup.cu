@@ -34,11 +34,14 @@ cudaError_t launch_build_thresholds(const uint32_t *counts, int V, float sample,
 __global__ void k_table_total(const double *pow_cn, int V, double *total_out) {
     const int lane = threadIdx.x;
     double total = 0.0;
-    for (int base = 0; base < V; base += 32) {
-        const double v = base + lane < V ? pow_cn[base + lane] : 0.0;
-        const int n = min(32, V - base);
-        for (int j = 0; j < n; j++) total += __shfl_sync(0xffffffffu, v, j);
+    int base = 0;
+    for (; base + 32 <= V; base += 32) {  // whole groups: unrolled, so the shuffles run ahead of the chain
+        const double v = pow_cn[base + lane];
+#pragma unroll
+        for (int j = 0; j < 32; j++) total += __shfl_sync(0xffffffffu, v, j);
     }
+    const double v = base + lane < V ? pow_cn[base + lane] : 0.0;
+    for (int j = 0; j < V - base; j++) total += __shfl_sync(0xffffffffu, v, j);
     if (lane == 0) *total_out = total;
 }
 
@@ -52,18 +55,26 @@ __global__ void k_table_quotients(const double *pow_cn, int V, const double *tot
 // d1 = (float) ((double) d1 + q_i), in index order; lane j keeps step j's value of each 32.
 __global__ void k_table_running(const double *q, int V, float *D) {
     const int lane = threadIdx.x;
-    float d1 = 0.f;
-    for (int base = 0; base < V; base += 32) {
-        const double v = base + lane < V ? q[base + lane] : 0.0;
-        const int n = min(32, V - base);
+    float d1 = (float) q[0];
+    if (lane == 0) D[0] = d1;
+    int base = 1;
+    for (; base + 32 <= V; base += 32) {  // whole groups: unrolled, so the shuffles run ahead of the chain
+        const double v = q[base + lane];
         float mine = 0.f;
-        for (int j = 0; j < n; j++) {
-            const double x = __shfl_sync(0xffffffffu, v, j);
-            d1 = base + j == 0 ? (float) x : (float) ((double) d1 + x);
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+            d1 = (float) ((double) d1 + __shfl_sync(0xffffffffu, v, j));
             if (lane == j) mine = d1;
         }
-        if (lane < n) D[base + lane] = mine;
+        D[base + lane] = mine;
     }
+    const double v = base + lane < V ? q[base + lane] : 0.0;
+    float mine = 0.f;
+    for (int j = 0; j < V - base; j++) {
+        d1 = (float) ((double) d1 + __shfl_sync(0xffffffffu, v, j));
+        if (lane == j) mine = d1;
+    }
+    if (base + lane < V) D[base + lane] = mine;
 }
 
 __device__ __forceinline__ float slot_position(int a) {  // a / (real) table_size
