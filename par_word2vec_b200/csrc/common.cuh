@@ -105,6 +105,17 @@ __device__ __forceinline__ float grad_from_table(float f, int label, float alpha
     return __fmul_rn(__fsub_rn((float) label, exp_table[idx]), alpha);
 }
 
+// Warp sum through one integer reduction (redux.sync): each lane's value is clamped to +-32 and
+// rounded to a multiple of 2^-20, so the 32 lanes add exactly and in any order, with no overflow
+// (32 x 32 x 2^20 = 2^30), and the result carries at most 32 x 2^-21 = 1.5e-5 absolute error.
+// One dependent step instead of five shuffles and adds.  For BF16 tables, whose rows are rounded
+// at 2^-9 relative, this is far below the storage precision (a dot product's inputs, not the
+// reduction, set its accuracy there); FP32 tables keep warp_sum.
+__device__ __forceinline__ float warp_sum_fixed(float v) {
+    const float c = fminf(fmaxf(v, -32.f), 32.f);
+    const int q = __float2int_rn(__fmul_rn(c, 1048576.f));
+    return __fmul_rn(__int2float_rn(__reduce_add_sync(0xffffffffu, q)), 1.f / 1048576.f);
+}
 __device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

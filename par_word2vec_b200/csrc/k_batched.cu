@@ -985,7 +985,7 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_stream_train(TrainArgs a
                             wc = __ldg(sen + c);
                             if (wc != word) xn = LR::load(w_in + (size_t) wc * ld, lane, vm);
                         }
-                        f = warp_sum(f);
+                        f = BF16 ? warp_sum_fixed(f) : warp_sum(f);
                         const float g = grad_from_table(f, 1, alpha, s_exp);
                         float xw[E];
                         LR::fma_scaled(g, y, xr, xw);  // from the entry values of y
